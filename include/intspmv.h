@@ -1,0 +1,294 @@
+/*
+ * intspmv.h - C ABI of int_spmv_b200, a B200 (sm_100a) SpMV library that is a
+ * drop-in for the C entry points and sparse formats of edoardoCB/int_spmv.
+ *
+ * Every reference citation below is `intSpmv_main.c:<line>` of that project
+ * (abbreviated `M:<line>`).  The reference is one C translation unit whose
+ * functions are all `static`; its "C entry points" are the signatures and
+ * struct layouts reproduced here, made non-static and `extern "C"`.
+ *
+ * Three layers:
+ *   1. Host format builders with the reference's signatures and allocation
+ *      contract (arrays malloc'd inside the struct, caller frees with free()).
+ *      Pointer, index and reorder arrays are bit-exact to the reference.
+ *      Status-returning `ispmv_build_*` forms sit beside the compat forms,
+ *      which, like the reference, print and exit(EXIT_FAILURE) on error.
+ *   2. Kernels with the reference's names and signatures on HOST pointers
+ *      (`cf_CSR`, `int_axc`, ...): each call copies its inputs to the GPU,
+ *      runs the sm_100a kernel and copies the result back.  `ompNT` is
+ *      accepted and ignored.  The same kernels on DEVICE pointers are the
+ *      `ispmv_dev_*` functions (stream-ordered, status-returning).
+ *   3. Plans (`ispmv_plan_*`): a format uploaded once to HBM as value and
+ *      column-index streams, then y = A*x (+ beta*y) for a fresh x on every
+ *      call, in FP64 or a reduced-byte form (FP32 values, FP64 accumulation).
+ *
+ * All functions returning `int` return an ISPMV_* status; 0 is success.
+ */
+#ifndef INTSPMV_H
+#define INTSPMV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------------
+ * Compile-time configuration of the reference (M:51-109, ic.sh:43).  Only the
+ * FP_TYPE=FP_DOUBLE build of the reference works (M:207 typo, `_pd`
+ * intrinsics), so FPT is double.
+ * ------------------------------------------------------------------------ */
+typedef double FPT;        /* M:63-73 */
+typedef unsigned int UIN;  /* M:77-79 */
+#define ISPMV_HBRICK_SIZE 8u /* M:101-103: brick / tile width */
+#define ISPMV_CHUNK_SIZE 8u  /* M:107-109: K1 chunk height */
+
+/* Status codes (the reference exits instead: M:171-179). */
+#define ISPMV_OK 0
+#define ISPMV_ERR_ARG 1         /* bad argument or malformed matrix */
+#define ISPMV_ERR_OOM 2         /* host or device allocation failed */
+#define ISPMV_ERR_CUDA 3        /* a CUDA runtime call failed */
+#define ISPMV_ERR_TIMEOUT 4     /* a bounded device wait gave up */
+#define ISPMV_ERR_UNSUPPORTED 5 /* valid for the reference, not implemented */
+#define ISPMV_ERR_OVERFLOW 6    /* a u32 length or index would overflow */
+
+/* ---------------------------------------------------------------------------
+ * Reference structs, field for field (same order, same types).
+ * ------------------------------------------------------------------------ */
+/* M:183 - input CSR plus row statistics; `rl` is filled by the stats pass
+ * (M:253-262).  rowStart/rowEnd are only used by the MKL rows (M:324-357). */
+typedef struct {
+  UIN nrows; UIN nnz; UIN rmin; FPT rave; UIN rmax; FPT rsd; UIN bw;
+  FPT *val; UIN *row; UIN *rowStart; UIN *rowEnd; UIN *col; UIN *rl;
+} str_matCSR;
+
+/* M:306 - per-format name, memory footprint [B], occupancy, conversion time */
+typedef struct { char name[24]; double mfp; double beta; double ct; } str_formatData;
+
+/* M:400 - error of a result against the CSR oracle (M:404-425) */
+typedef struct { double aErr; double rErr; UIN pos; } str_err;
+
+/* M:429 - one row of the kernels' results table */
+typedef struct { char name[25]; double et; double ot; double flops; str_err sErr; } str_res;
+
+/* M:615 - AXC: rows of 8-wide bricks, each 8 values then 8 x copies */
+typedef struct { UIN nrows; UIN nnz; UIN lenAX; UIN lenBRP; FPT *ax; UIN *brp; } str_matAXC;
+
+/* M:771 - K1: rows sorted by length, 8-row chunks stored column-major */
+typedef struct {
+  UIN nrows; UIN nnz; UIN chunkNum; UIN lenVC;
+  UIN *permi; UIN *nmc; UIN *chp; FPT *val; UIN *col;
+} str_matK1;
+
+/* M:1114 - AXT: tiles of tileH sub-rows x (8 values + 8 x copies) */
+typedef struct {
+  UIN nrows; UIN nnz; char mode[8]; UIN tileHW; UIN tileH; UIN logTH; UIN tileN;
+  UIN lenAX; UIN lenSEC; UIN lenCON; UIN log; FPT *ax; UIN *sec; UIN *con;
+} str_matAXT;
+
+/* ---------------------------------------------------------------------------
+ * Layer 1: host format builders.
+ * ------------------------------------------------------------------------ */
+
+/* Fills rl[i] = row[i+1]-row[i] and rmin/rave/rmax/rsd/bw of `csr`
+ * (the computation of printMatrixStats, M:253-278, without its .sta file).
+ * Also validates the CSR (row pointers monotone, row[n]==nnz, col<nrows). */
+int ispmv_csr_stats(str_matCSR *csr);
+
+/* printMatrixStats, M:253-302: ispmv_csr_stats plus the `<name>.sta` file,
+ * written beside the matrix file (the extension after the last '.' of the
+ * file name is replaced; the reference's strtok rule breaks on dotted paths,
+ * M:280-287). */
+void printMatrixStats(const char *matFileName, str_matCSR *matCSR);
+
+/* matrixReading, M:187-249: reads a `.csr` text file ("n nnz", nnz lines
+ * "val col", n+1 row pointers) or a `.bin` file (u32 n, u32 nnz, FPT
+ * val[nnz], u32 col[nnz], u32 row[n+1]).  Arrays are malloc'd, rl included
+ * (unfilled until the stats pass).  ispmv_matrix_read returns a status;
+ * matrixReading exits on error like the reference. */
+int ispmv_matrix_read(const char *matFileName, str_matCSR *out);
+str_matCSR matrixReading(const char *matFileName);
+/* Writes `csr` as a .csr (text) or .bin file, chosen by the extension. */
+int ispmv_matrix_write(const char *matFileName, const str_matCSR *csr);
+/* Frees every array of a CSR produced by ispmv_matrix_read. */
+void ispmv_csr_free(str_matCSR *csr);
+
+/* getFormatDataCSR, M:324-357: rowStart/rowEnd copies and the CSR row of
+ * the formats table (memory footprint includes the x vector, M:350). */
+int ispmv_build_csr(str_matCSR *csr, str_formatData *fd);
+str_formatData getFormatDataCSR(str_matCSR *matCSR);
+
+/* getFormatDataAXC, M:662-707.  brp (M:619-628) is calloc'd, ax (M:632-658)
+ * is 64-byte aligned with its padding zeroed.  Requires csr.rl. */
+int ispmv_build_axc(UIN ompNT, const str_matCSR *csr, const FPT *vec, str_matAXC *out,
+                    str_formatData *fd);
+str_formatData getFormatDataAXC(const UIN ompNumThreads, const str_matCSR matCSR,
+                                const FPT *vec, str_matAXC *matAXC);
+
+/* getFormatDataK1, M:841-905.  permi (M:782-796) orders rows by length
+ * descending, ties by ascending row id (the order glibc's qsort gives the
+ * reference, M:775-778); nmc/chp (M:800-813); val/col (M:817-837) padding
+ * zeroed.  `blockSize` is unused, as in the reference. */
+int ispmv_build_k1(UIN blockSize, const str_matCSR *csr, const FPT *vec, str_matK1 *out,
+                   str_formatData *fd);
+str_formatData getFormatDataK1(const UIN blockSize, const str_matCSR matCSR,
+                               const FPT *vec, str_matK1 *matK1);
+
+/* getFormatDataAXT, M:1275-1381.  mode "NOC" (uncompacted, any tileH >= 1)
+ * or "COM" (compacted, tileH == 1 and bs a power of two in [2, 512]; the
+ * reference leaves COM with tileH > 1 unimplemented, M:1338-1362).
+ * con (M:1118-1148), ax and sec (M:1152-1260) are bit-exact; ax and sec
+ * padding is zero (M:1304-1305). */
+int ispmv_build_axt(UIN ompNT, UIN bs, UIN thw, UIN th, const char *mode,
+                    const str_matCSR *csr, const FPT *vec, str_matAXT *out,
+                    str_formatData *fd);
+str_formatData getFormatDataAXT(const UIN ompNT, const UIN bs, const UIN thw, const UIN th,
+                                const char *mode, const str_matCSR matCSR, const FPT *vec,
+                                str_matAXT *matAXT);
+
+/* Column-index companions (no reference counterpart): the reference bakes
+ * x into ax (M:644, M:1171, M:1207, M:1247), so its AXC/AXT kernels never
+ * gather x.  The companion holds, for every value slot of ax, the column of
+ * that value: axi[s] is the column of ax[(s/thw)*2*thw + s%thw];
+ * length lenAX/2; padding slots hold column 0 (their value is 0.0).
+ * *axi is malloc'd; the caller frees it. */
+int ispmv_build_axc_cols(UIN ompNT, const str_matCSR *csr, const str_matAXC *axc, UIN **axi);
+int ispmv_build_axt_cols(UIN ompNT, const str_matCSR *csr, const str_matAXT *axt, UIN **axi);
+
+/* Frees the arrays a builder allocated and zeroes the struct. */
+void ispmv_free_axc(str_matAXC *m);
+void ispmv_free_k1(str_matK1 *m);
+void ispmv_free_axt(str_matAXT *m);
+
+/* getErrors, M:404-425: aErr = max_i | |res_i| - |ref_i| |, rErr = aErr /
+ * max_i |ref_i|, pos = first argmax. */
+void getErrors(const UIN len, const FPT *ar, const FPT *ac, str_err *sErr);
+void initVec(const UIN len, FPT *vec); /* M:361-367: vec[i] = i */
+
+/* ---------------------------------------------------------------------------
+ * Layer 2a: kernels on DEVICE pointers (stream-ordered; `stream` is a
+ * cudaStream_t, NULL for the legacy default stream).  Same arithmetic and
+ * accumulation contract as the reference kernel each one replaces; AXT
+ * kernels accumulate into y (the caller zeroes it, M:1421,1492,1591).
+ * ------------------------------------------------------------------------ */
+int ispmv_dev_cf_csr(UIN nrows, const UIN *row, const UIN *col, const FPT *val, const FPT *vec,
+                     FPT *res, void *stream);                                   /* M:382 */
+int ispmv_dev_int_axc(UIN nrows, const FPT *ax, const UIN *brp, FPT *y, void *stream); /* M:711 */
+int ispmv_dev_int_k1(UIN chunkNum, const FPT *val, const UIN *col, const UIN *chp,
+                     const UIN *nmc, const FPT *vec, FPT *res, void *stream);   /* M:943 */
+int ispmv_dev_order_k1(UIN len, const UIN *permi, const FPT *arrDis, FPT *arrOrd,
+                       void *stream);                                           /* M:969 */
+/* `mask` is the reference's tail mask for the last chunk (M:1077-1086):
+ * bit i set = lane i of the last chunk is a real row. */
+int ispmv_dev_int_k1p(unsigned char mask, UIN chunkNum, const FPT *val, const UIN *col,
+                      const UIN *chp, const UIN *nmc, const UIN *permi, const FPT *vec,
+                      FPT *res, void *stream);                                  /* M:1026 */
+int ispmv_dev_int_axt_noc_h1(UIN tileNum, const FPT *ax, const UIN *rwp, FPT *y,
+                             void *stream);                                     /* M:1385 */
+int ispmv_dev_int_axt_noc(UIN tileNum, UIN tileHeight, const FPT *ax, const UIN *rwp, FPT *y,
+                          void *stream);                                        /* M:1443 */
+/* Compacted AXT (M:1517).  Computes the true segmented sum of every
+ * segment, including row-0 segments whose descriptor encodes as 0 (the
+ * reference skips those, M:1555) and without reading past lenAX. */
+int ispmv_dev_int_axt_com_h1(UIN bn, UIN bs, UIN log, UIN thw, UIN tn, UIN lenAX, UIN lenRWP,
+                             const FPT *ax, const UIN *rwp, FPT *y, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Layer 2b: the reference's kernels by name on HOST pointers.  Each call
+ * copies its inputs to the current GPU, runs the ispmv_dev_* kernel and
+ * copies the result back (synchronous).  Errors print and exit, as the
+ * reference does.  `ompNT` is ignored.
+ * ------------------------------------------------------------------------ */
+void cf_CSR(const str_matCSR matCSR, const FPT *vec, FPT *res);                 /* M:382 */
+void int_axc(const UIN ompNT, const UIN nrows, const FPT *ax, const UIN *brp, FPT *y); /* M:711 */
+void int_k1(const UIN ompNT, const UIN chunkNum, const FPT *val, const UIN *col,
+            const UIN *chp, const UIN *nmc, const FPT *vec, FPT *res);         /* M:943 */
+void orderArrayK1(const UIN ompNT, const UIN len, const UIN *permi, const FPT *arrDis,
+                  FPT *arrOrd);                                                 /* M:969 */
+void int_k1p(const UIN ompNT, const unsigned char mask, const UIN chunkNum, const FPT *val,
+             const UIN *col, const UIN *chp, const UIN *nmc, const UIN *permi,
+             const FPT *vec, FPT *res);                                         /* M:1026 */
+void int_axt_noc_h1(const UIN ompNT, const UIN tileNum, const FPT *ax, const UIN *rwp,
+                    FPT *y);                                                    /* M:1385 */
+void int_axt_noc(const UIN ompNT, const UIN tileNum, const UIN tileHeight, const FPT *ax,
+                 const UIN *rwp, FPT *y);                                       /* M:1443 */
+void int_axt_com_h1(const UIN ompNT, const UIN bn, const UIN bs, const UIN log, const UIN thw,
+                    const UIN tn, const UIN lenAX, const UIN lenRWP, const FPT *ax,
+                    const UIN *rwp, FPT *y);                                    /* M:1517 */
+
+/* ---------------------------------------------------------------------------
+ * Layer 3: plans - a format resident in HBM as value/column streams; every
+ * call gathers a fresh x through L2.  No reference counterpart: the
+ * reference rebuilds ax for every new x (its conversion time).
+ * ------------------------------------------------------------------------ */
+typedef struct ispmv_plan_s *ispmv_plan;
+
+/* Value storage of a plan.  Accumulation is FP64 in every form. */
+#define ISPMV_VAL_F64 0      /* FP64 values (the drop-in) */
+#define ISPMV_VAL_F32 1      /* FP32 values, FP32 multiply, FP64 accumulate */
+#define ISPMV_VAL_F32_LO16 2 /* FP32 + BF16 residual lo-word on rows that need it */
+/* Column storage of a plan. */
+#define ISPMV_COL_U32 0      /* exact u32 columns */
+#define ISPMV_COL_D16 1      /* 16-bit deltas from a per-unit base column */
+
+/* Kernel variants a plan can run (ispmv_plan_opts.kernel). */
+#define ISPMV_KERNEL_AUTO 0
+#define ISPMV_KERNEL_LDG 1   /* register-streaming loads */
+#define ISPMV_KERNEL_TMA 2   /* 1D bulk copies (cp.async.bulk) into shared memory */
+
+typedef struct {
+  int val_kind;      /* ISPMV_VAL_* */
+  int col_kind;      /* ISPMV_COL_* */
+  int kernel;        /* ISPMV_KERNEL_* */
+  int ctas_per_sm;   /* 0 = library default */
+  int units_per_warp;/* work granule of one warp; 0 = library default */
+  double lo_tol;     /* F32_LO16: rows whose FP32 rounding error bound exceeds
+                        lo_tol relative carry a lo-word; 0 = default 1e-9 */
+} ispmv_plan_opts;
+
+void ispmv_plan_opts_default(ispmv_plan_opts *o);
+
+/* Plans from host-built formats.  The host arrays are only read during the
+ * call; the plan owns its device copies.  `csr` must have rl filled. */
+int ispmv_plan_csr(const str_matCSR *csr, const ispmv_plan_opts *o, ispmv_plan *out);
+int ispmv_plan_axc(const str_matCSR *csr, const str_matAXC *axc, const UIN *axi,
+                   const ispmv_plan_opts *o, ispmv_plan *out);
+/* reorder: 0 = int_k1 (result in chunk order, then orderArrayK1),
+ *          1 = int_k1p (reordering integrated, scatter to y[permi]). */
+int ispmv_plan_k1(const str_matCSR *csr, const str_matK1 *k1, int reorder,
+                  const ispmv_plan_opts *o, ispmv_plan *out);
+int ispmv_plan_axt(const str_matCSR *csr, const str_matAXT *axt, const UIN *axi,
+                   const ispmv_plan_opts *o, ispmv_plan *out);
+int ispmv_plan_destroy(ispmv_plan p);
+
+/* y = A*x + beta*y with device pointers, beta in {0, 1}.  Stream-ordered. */
+int ispmv_plan_spmv(ispmv_plan p, const FPT *x, FPT *y, int beta, void *stream);
+/* Y = A*X for k right-hand sides, X and Y row-major (n x k), FP64. */
+int ispmv_plan_spmm(ispmv_plan p, UIN k, const FPT *X, FPT *Y, void *stream);
+/* End to end on HOST buffers: copies x in, runs the SpMV, copies y out and
+ * synchronises `stream`.  Pinned host buffers give full PCIe bandwidth. */
+int ispmv_plan_spmv_host(ispmv_plan p, const FPT *h_x, FPT *h_y, void *stream);
+
+/* Plan facts: rows, nonzeros, value slots streamed, bytes of device
+ * storage, and the algorithmic bytes of one SpMV:
+ * nnz*(b_val + b_idx) + n*(b_x + b_y) + 4*(n+1). */
+typedef struct {
+  UIN nrows; UIN nnz; uint64_t slots; uint64_t device_bytes; double alg_bytes;
+  int format; int val_kind; int col_kind; int kernel; UIN tile_h; UIN bs;
+  char name[32];
+} ispmv_plan_info;
+int ispmv_plan_get_info(ispmv_plan p, ispmv_plan_info *info);
+
+/* Library facts and diagnostics. */
+const char *ispmv_version(void);
+const char *ispmv_status_string(int status);
+/* Last CUDA error text seen by the library on this thread ("" if none). */
+const char *ispmv_last_error(void);
+/* Kernel launches issued by the library since load (all ispmv_* calls). */
+unsigned long long ispmv_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* INTSPMV_H */

@@ -1,0 +1,234 @@
+// plan_kernels.cuh - sm_100a SpMV kernels of the plan layer (fresh x per
+// call, gathered through the read-only path / L2; values and columns are
+// streamed once with evict-first loads).
+//
+// VT is the stored value type (double, or float for the reduced-byte form:
+// FP32 multiply, FP64 accumulation).
+#pragma once
+#include "seg_engine.cuh"
+
+namespace ispmv {
+namespace pk {
+
+constexpr int TPB = 256;
+
+template <typename VT>
+__device__ __forceinline__ double prod(VT v, double x);
+template <>
+__device__ __forceinline__ double prod<double>(double v, double x) { return v * x; }
+template <>
+__device__ __forceinline__ double prod<float>(float v, double x) { return (double)(v * __double2float_rn(x)); }
+
+template <typename VT>
+__device__ __forceinline__ double fmac(VT v, double x, double acc);
+template <>
+__device__ __forceinline__ double fmac<double>(double v, double x, double acc) { return fma(v, x, acc); }
+template <>
+__device__ __forceinline__ double fmac<float>(float v, double x, double acc) {
+  return acc + (double)(v * __double2float_rn(x));
+}
+
+// ---------------------------------------------------------------- CSR --
+// Vector CSR ("naive" CSR on the GPU): L lanes per row, shuffle reduction,
+// overwrite / accumulate y.
+template <typename VT, int L>
+__global__ void __launch_bounds__(TPB) csr_vec(UIN n, const UIN *__restrict__ row, const UIN *__restrict__ col,
+                                               const VT *__restrict__ val, const FPT *__restrict__ x,
+                                               FPT *__restrict__ y, int beta) {
+  const unsigned sub = threadIdx.x & (L - 1);
+  const size_t r = ((size_t)blockIdx.x * TPB + threadIdx.x) / L;
+  const bool live = r < n;
+  double s = 0.0;
+  if (live) {
+    const UIN b = row[r], e = row[r + 1];
+    for (UIN j = b + sub; j < e; j += L) s = fmac<VT>(ld_stream(val + j), ldg(x + ld_stream(col + j)), s);
+  }
+#pragma unroll
+  for (int d = L / 2; d > 0; d >>= 1) s += __shfl_xor_sync(FULL, s, d);
+  if (live && sub == 0) y[r] = beta ? s + y[r] : s;
+}
+
+// ---------------------------------------------------------------- AXC --
+// 8 lanes per row, one 8-value brick per step (the reference's row loop,
+// M:711-732, with x gathered from the column companion).
+template <typename VT>
+__global__ void __launch_bounds__(TPB) axc_rows(UIN n, const UIN *__restrict__ bptr, const UIN *__restrict__ col,
+                                                const VT *__restrict__ val, const FPT *__restrict__ x,
+                                                FPT *__restrict__ y, int beta) {
+  const unsigned k = threadIdx.x & 7u;
+  const size_t r = ((size_t)blockIdx.x * TPB + threadIdx.x) >> 3;
+  const bool live = r < n;
+  double s = 0.0;
+  if (live) {
+    const size_t b = (size_t)bptr[r] * 8, e = (size_t)bptr[r + 1] * 8;
+    for (size_t p = b + k; p < e; p += 8) s = fmac<VT>(ld_stream(val + p), ldg(x + ld_stream(col + p)), s);
+  }
+  s += __shfl_xor_sync(FULL, s, 4);
+  s += __shfl_xor_sync(FULL, s, 2);
+  s += __shfl_xor_sync(FULL, s, 1);
+  if (live && k == 0) y[r] = beta ? s + y[r] : s;
+}
+
+// ----------------------------------------------------------------- K1 --
+// 8 lanes per chunk; SCATTER writes y[permi] (K1 with integrated
+// reordering), else res in chunk order (then k1_order).
+template <typename VT, bool SCATTER>
+__global__ void __launch_bounds__(TPB) k1_chunks(UIN n, UIN chunkNum, const UIN *__restrict__ chp,
+                                                 const UIN *__restrict__ nmc, const UIN *__restrict__ permi,
+                                                 const UIN *__restrict__ col, const VT *__restrict__ val,
+                                                 const FPT *__restrict__ x, FPT *__restrict__ out, int beta) {
+  const unsigned lane8 = threadIdx.x & 7u;
+  const size_t c = ((size_t)blockIdx.x * TPB + threadIdx.x) >> 3;
+  if (c >= chunkNum) return;
+  const size_t off = chp[c];
+  const UIN m = nmc[c];
+  double s0 = 0.0, s1 = 0.0;
+  UIN k = 0;
+  for (; k + 1 < m; k += 2) {
+    const size_t p = off + (size_t)k * 8 + lane8;
+    s0 = fmac<VT>(ld_stream(val + p), ldg(x + ld_stream(col + p)), s0);
+    s1 = fmac<VT>(ld_stream(val + p + 8), ldg(x + ld_stream(col + p + 8)), s1);
+  }
+  if (k < m) {
+    const size_t p = off + (size_t)k * 8 + lane8;
+    s0 = fmac<VT>(ld_stream(val + p), ldg(x + ld_stream(col + p)), s0);
+  }
+  const double s = s0 + s1;
+  const size_t i = c * 8 + lane8;
+  if (SCATTER) {
+    if (i < n) {
+      const UIN r = permi[i];
+      out[r] = beta ? s + out[r] : s;
+    }
+  } else {
+    out[i] = s;
+  }
+}
+
+__global__ void k1_order(UIN n, const UIN *__restrict__ permi, const FPT *__restrict__ res, FPT *__restrict__ y,
+                         int beta) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    const UIN r = permi[i];
+    y[r] = beta ? res[i] + y[r] : res[i];
+  }
+}
+
+// ------------------------------------------------------- AXT NOC, th=1 --
+// Unit = tile of 8 slots of one row (row id: sec).  Each step 8 lanes load
+// one tile (32 lanes = 4 tiles: coalesced 256-byte value loads), reduce it
+// with 3 shuffles, and lane u of the batch collects tile u's sum.
+template <typename VT>
+__global__ void __launch_bounds__(TPB) noc_h1(size_t nunits, UIN useg, const UIN *__restrict__ urow,
+                                              const UIN *__restrict__ col, const VT *__restrict__ val,
+                                              const FPT *__restrict__ x, seg::Out o) {
+  const unsigned lane = threadIdx.x & 31u;
+  const size_t segid = ((size_t)blockIdx.x * TPB + threadIdx.x) >> 5;
+  const size_t u0 = segid * useg;
+  if (u0 >= nunits) return;
+  const size_t u1 = min(u0 + useg, nunits);
+  seg::State st{NO_ROW, 0.0, false};
+  for (size_t ub = u0; ub < u1; ub += 32) {
+    double mine = 0.0;
+#pragma unroll 4
+    for (int j = 0; j < 8; j++) {
+      const size_t t = ub + (size_t)j * 4 + (lane >> 3);
+      double p = 0.0;
+      if (t < u1) {
+        const size_t q = t * 8 + (lane & 7u);
+        p = prod<VT>(ld_stream(val + q), ldg(x + ld_stream(col + q)));
+      }
+      p += __shfl_xor_sync(FULL, p, 4);
+      p += __shfl_xor_sync(FULL, p, 2);
+      p += __shfl_xor_sync(FULL, p, 1);
+      const double tsum = __shfl_sync(FULL, p, (lane & 3u) * 8);
+      if ((lane >> 2) == (unsigned)j) mine = tsum;
+    }
+    const size_t u = ub + lane;
+    const bool live = u < u1;
+    const UIN r = live ? urow[u] : NO_ROW;
+    seg::batch(mine, r, live, st, o, segid);
+  }
+  seg::finish(st, o, segid);
+}
+
+// ------------------------------------------------------- AXT NOC, th>1 --
+// Unit = tile column of th slots (row id: sec[8*T + c]).  th % 4 == 0: each
+// step the warp loads 4 consecutive sub-rows of a tile (32 consecutive
+// slots), adds them per column, and after th/4 steps reduces the 4 partials
+// of each column with 2 shuffles; 4 tiles make a batch of 32 columns.
+template <typename VT>
+__global__ void __launch_bounds__(TPB) noc_hn(size_t nunits, UIN th, UIN useg, const UIN *__restrict__ urow,
+                                              const UIN *__restrict__ col, const VT *__restrict__ val,
+                                              const FPT *__restrict__ x, seg::Out o) {
+  const unsigned lane = threadIdx.x & 31u;
+  const size_t segid = ((size_t)blockIdx.x * TPB + threadIdx.x) >> 5;
+  const size_t u0 = segid * useg;  // useg is a multiple of 32 (4 tiles)
+  if (u0 >= nunits) return;
+  const size_t u1 = min(u0 + useg, nunits);
+  seg::State st{NO_ROW, 0.0, false};
+  const size_t tslots = (size_t)th * 8;
+  for (size_t ub = u0; ub < u1; ub += 32) {
+    double mine = 0.0;
+    for (int tt = 0; tt < 4; tt++) {
+      const size_t T = ub / 8 + tt;
+      double p = 0.0;
+      if (T * 8 < u1) {
+        const size_t base = T * tslots + lane;
+        if (th % 4 == 0) {
+          for (UIN R = 0; R < th; R += 4) {
+            const size_t q = base + (size_t)R * 8;
+            p = fmac<VT>(ld_stream(val + q), ldg(x + ld_stream(col + q)), p);
+          }
+        } else {
+          // generic tileH: lane = (group g = lane/8, column c): sub-rows g, g+4, ...
+          for (UIN R = lane >> 3; R < th; R += 4) {
+            const size_t q = T * tslots + (size_t)R * 8 + (lane & 7u);
+            p = fmac<VT>(ld_stream(val + q), ldg(x + ld_stream(col + q)), p);
+          }
+        }
+      }
+      p += __shfl_xor_sync(FULL, p, 8);
+      p += __shfl_xor_sync(FULL, p, 16);
+      if ((lane >> 3) == (unsigned)tt) mine = p;
+    }
+    const size_t u = ub + lane;
+    const bool live = u < u1;
+    const UIN r = live ? urow[u] : NO_ROW;
+    seg::batch(mine, r, live, st, o, segid);
+  }
+  seg::finish(st, o, segid);
+}
+
+// ----------------------------------------------------------- AXT COM --
+// Unit = slot (packed, CSR order).  Row starts are a bitmap (bit s of
+// heads = a non-empty row starts at slot s); the compressed row of slot s
+// is (#starts <= s) - 1, counted from the segment's base `segh`.
+template <typename VT>
+__global__ void __launch_bounds__(TPB) com_slots(size_t nslots, UIN useg, const UIN *__restrict__ heads,
+                                                 const UIN *__restrict__ segh, const UIN *__restrict__ col,
+                                                 const VT *__restrict__ val, const FPT *__restrict__ x,
+                                                 seg::Out o) {
+  const unsigned lane = threadIdx.x & 31u;
+  const size_t segid = ((size_t)blockIdx.x * TPB + threadIdx.x) >> 5;
+  const size_t s0 = segid * useg;  // multiple of 32
+  if (s0 >= nslots) return;
+  const size_t s1 = min(s0 + useg, nslots);
+  seg::State st{NO_ROW, 0.0, false};
+  UIN cnt = segh[segid];
+  const unsigned le = (lane == 31) ? FULL : ((2u << lane) - 1u);
+  for (size_t sb = s0; sb < s1; sb += 32) {
+    const size_t s = sb + lane;
+    const bool live = s < s1;
+    double p = 0.0;
+    if (live) p = prod<VT>(ld_stream(val + s), ldg(x + ld_stream(col + s)));
+    const UIN w = heads[sb >> 5];
+    const UIN r = live ? cnt + __popc(w & le) - 1u : NO_ROW;
+    cnt += __popc(w);
+    seg::batch(p, r, live, st, o, segid);
+  }
+  seg::finish(st, o, segid);
+}
+
+}  // namespace pk
+}  // namespace ispmv
