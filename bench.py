@@ -1,0 +1,407 @@
+"""SpMV throughput on one B200 (or N, one process per GPU): the power-law
+workload (n = 4,000,000; lognormal(2.2, 1.0) row lengths; 70% of each row's
+columns in a +/-1000 band, 30% uniform; seed 1), FP64.
+
+One step = one y = A x through a plan (the format resident in HBM, x gathered
+through L2).  The headline format is the compacted AXT (AXT COM, bs 128).
+Inputs are larger than L2 (~0.8 GB streamed per step), so no flush is needed.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--format COM128] [--workload powerlaw4m|poisson512|stencil160]
+                    [--no-formats] [--no-cpu]
+
+`--impl reference` times the reference's own CPU kernel (edoardoCB/int_spmv
+intSpmv_main.c, compiled from its own source into oracle/_ref) for the same
+format on the host cores, each step a bounded row sample of the workload.
+Prints ONE JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "SpMV GFLOP/s"
+UNIT = "GFLOP/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+# ------------------------------------------------------------- workloads --
+def make_workload(name: str):
+    from int_spmv_b200 import matrices as M
+    if name == "powerlaw4m":
+        row, col, val = M.powerlaw(4_000_000, seed=1)
+        return dict(name="powerlaw_n4M_seed1", row=row, col=col, val=val, x=M.uniform_x(4_000_000, 1),
+                    desc="power-law n=4,000,000, rl=clip(rint(lognormal(2.2,1.0)),1,5000), 70% band +/-1000, "
+                         "30% uniform, N(0,1) values, x~U[-1,1], seed 1")
+    if name == "poisson512":
+        row, col, val = M.poisson2d(512)
+        return dict(name="poisson2d_512", row=row, col=col, val=val, x=M.uniform_x(512 * 512, 0),
+                    desc="2D 5-point Poisson 512x512, natural order, x~U[-1,1] seed 0")
+    if name == "stencil160":
+        row, col, val = M.stencil27(160, seed=2)
+        return dict(name="stencil27_160", row=row, col=col, val=val, x=M.uniform_x(160 ** 3, 2),
+                    desc="3D 27-point stencil 160^3, diag 26, off -1+U[-0.1,0.1], seed 2")
+    raise ValueError(name)
+
+
+def build_format(F, csr, x, fmt: str):
+    """fmt: CSR | AXC | K1 | K1P | NOC<th> | COM<bs>.  Returns the host format
+    object (None for CSR) and the reference format name."""
+    if fmt == "CSR":
+        return None, "CSR"
+    if fmt == "AXC":
+        return F.getFormatDataAXC(0, csr, x)[1], "AXC"
+    if fmt in ("K1", "K1P"):
+        return F.getFormatDataK1(8, csr, x)[1], fmt
+    if fmt.startswith("NOC"):
+        th = int(fmt[3:])
+        return F.getFormatDataAXT(0, 128, 8, th, "NOC", csr, x)[1], f"AXT_NOC_H{th}_HW8"
+    if fmt.startswith("COM"):
+        bs = int(fmt[3:])
+        return F.getFormatDataAXT(0, bs, 8, 1, "COM", csr, x)[1], f"AXT_COM_H1_HW8_BS{bs}"
+    raise ValueError(fmt)
+
+
+def alg_bytes(n: int, nnz: int, bval: int = 8) -> float:
+    """nnz*(b_val + b_idx) + n*(b_x + b_y) + 4*(n+1)."""
+    return nnz * (bval + 4.0) + n * 16.0 + 4.0 * (n + 1)
+
+
+# --------------------------------------------------------------- helpers --
+def hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
+
+
+def traffic_for(kernel_key: str):
+    """dram bytes per launch from a committed ncu summary, if one exists."""
+    p = ROOT / "profiles" / "ncu_traffic.json"
+    try:
+        d = json.loads(p.read_text())
+        return d.get(kernel_key)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled in the background."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int, period_ms: int = 100):
+        self.samples, self.proc, self.t = [], None, None
+        self.gpu, self.period = gpu_index, period_ms
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", str(self.period)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.t = threading.Thread(target=self._read, daemon=True)
+        self.t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append((time.time(), [s.strip() for s in line.split(",")]))
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self, t0: float, t1: float):
+        win = [s for t, s in self.samples if t0 <= t <= t1] or [s for _, s in self.samples]
+        if not win:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        sm = [float(s[1]) for s in win if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in win if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in win for i in range(4) if len(s) > 5 + i and s[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(win),
+                "power_w_max": max(float(s[3]) for s in win if s[3].replace(".", "").isdigit()) if win else None}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0")), ws
+
+
+def max_over_ranks(v: float, ws: int, device=None) -> float:
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def timed(step, steps: int, warmup: int, ws: int, stream, device=None):
+    """W untimed steps, then exactly K steps between barrier + synchronize,
+    timed with CUDA events on `stream`; returns the max over ranks [s]."""
+    import torch
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(ws)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t_wall0 = time.time()
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_wall1 = time.time()
+    barrier(ws)
+    sec = e0.elapsed_time(e1) / 1e3
+    return max_over_ranks(sec, ws, device), (t_wall0, t_wall1)
+
+
+# ------------------------------------------------------- reference (CPU) --
+def reference_time(row, col, val, x, fmt: str, budget_s: float, calls: int | None = None, row_frac: float = 1.0,
+                   warm: int = 1):
+    """The reference's own kernel for `fmt` on the host cores: builds the
+    reference format with the reference builder, then times its kernel
+    (its gettimeofday timing).  Returns (sec/call, nnz of the sample, info)."""
+    from oracle import Reference
+    R = Reference()
+    n = len(row) - 1
+    nr = max(1, int(n * row_frac))
+    srow = row[:nr + 1]
+    snnz = int(srow[-1])
+    s = R.csr(srow, col[:snnz], val[:snnz])
+    s._keep[3][:] = np.diff(srow)
+    cores = os.cpu_count() or 1
+    kind, mat, bs, work = None, None, 0, 0
+    if fmt == "CSR":
+        kind, mat = "cf_CSR", s
+        cores = 1  # the reference's cf_CSR is serial (intSpmv_main.c:386)
+    elif fmt == "AXC":
+        d = R.build_axc(s, x, ompNT=cores)
+        kind, mat = "int_axc", d["struct"]
+    elif fmt in ("K1", "K1P"):
+        d = R.build_k1(s, x)
+        kind, mat, work = ("int_k1" if fmt == "K1" else "int_k1p"), d["struct"], d["chunkNum"] * 8
+    elif fmt.startswith("NOC"):
+        th = int(fmt[3:])
+        d = R.build_axt(s, x, 8, th, "NOC", 128, ompNT=cores)
+        kind, mat = ("int_axt_noc_h1" if th == 1 else "int_axt_noc"), d["struct"]
+    else:
+        bs = int(fmt[3:])
+        d = R.build_axt(s, x, 8, 1, "COM", bs, ompNT=cores)
+        kind, mat = "int_axt_com_h1", d["struct"]
+    et, _, _ = R.time_kernel(kind, mat, x, nr, work_len=work, bs=bs, iters=max(1, warm), ompNT=cores)
+    if calls is None:
+        calls = int(max(3, min(200, budget_s / max(et, 1e-6))))
+    et, ot, _ = R.time_kernel(kind, mat, x, nr, work_len=work, bs=bs, iters=calls, ompNT=cores)
+    if fmt == "K1":
+        et += ot
+    return et, snnz, dict(kernel=kind, calls=calls, cores=cores, rows=nr)
+
+
+# ------------------------------------------------------------------ main --
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=6000)
+    ap.add_argument("--warmup", type=int, default=100)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="powerlaw4m")
+    ap.add_argument("--format", default="COM128")
+    ap.add_argument("--no-formats", action="store_true", help="skip the per-format table")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of reference CPU work")
+    a = ap.parse_args(argv)
+    rank, local_rank, ws = dist_env()
+    W = max(3, a.warmup)
+
+    if a.impl == "reference":
+        return main_reference(a, rank, ws, W)
+
+    import torch
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+
+    from int_spmv_b200 import _lib
+    from int_spmv_b200 import device as D
+    from int_spmv_b200 import formats as F
+    wl = make_workload(a.workload)
+    csr = F.CSR(wl["row"], wl["col"], wl["val"])
+    n, nnz = csr.n, csr.nnz
+    fmt_obj, fmt_name = build_format(F, csr, wl["x"], a.format)
+    plan = D.Plan(csr, fmt_obj)
+    del fmt_obj
+    stream = torch.cuda.current_stream()
+    x = torch.from_numpy(wl["x"]).to(dev)
+    y = torch.empty(n, dtype=torch.float64, device=dev)
+    flops = 2.0 * nnz
+    B = alg_bytes(n, nnz)
+
+    l0 = _lib.launch_count()
+    plan.spmv(x, y)
+    per_step = _lib.launch_count() - l0  # library kernel launches in one step
+    try:
+        gpu_id = "GPU-" + str(torch.cuda.get_device_properties(local_rank).uuid)
+    except Exception:
+        gpu_id = str(local_rank)
+    sampler = ClockSampler(gpu_id)
+    sampler.start()
+    time.sleep(0.3)
+    sec, (tw0, tw1) = timed(lambda: plan.spmv(x, y), a.steps, W, ws, stream, dev)
+    time.sleep(0.25)
+    sampler.stop()
+    clocks = sampler.summary(tw0, tw1)
+    ms = sec / a.steps * 1e3
+    value = ws * a.steps * flops / sec / 1e9
+    gbs = B / (sec / a.steps) / 1e9
+    peak, peak_src = hbm_peak()
+
+    # end to end through the public API on pinned host buffers
+    hx = torch.from_numpy(wl["x"].copy()).pin_memory()
+    hy = torch.empty(n, dtype=torch.float64).pin_memory()
+    e2e_steps = max(3, min(a.steps, 300))
+    sec_e2e, _ = timed(lambda: plan.spmv_host(hx, hy), e2e_steps, 3, ws, stream, dev)
+    e2e = {"value": ws * e2e_steps * flops / sec_e2e / 1e9, "unit": UNIT, "h2d_bytes_per_step": 8 * n,
+           "d2h_bytes_per_step": 8 * n, "steps": e2e_steps, "ms_per_step": sec_e2e / e2e_steps * 1e3}
+
+    # parity of this run's y against the oracle (the checker, not the product)
+    check = None
+    if rank == 0:
+        from oracle import Oracle
+        orc = Oracle()
+        plan.spmv(x, y)
+        yr = orc.cf_csr(wl["row"], wl["col"], wl["val"], wl["x"])
+        ab = orc.abs_csr(wl["row"], wl["col"], wl["val"], wl["x"])
+        err = np.abs(y.cpu().numpy() - yr)
+        check = {"max_componentwise": float(np.max(err / np.maximum(ab, 1e-300))), "bound": 1e-12,
+                 "pass": bool(np.all(err <= 1e-12 * ab))}
+
+    formats = {}
+    if not a.no_formats:
+        for f in ["CSR", "AXC", "K1", "K1P", "NOC1", "NOC4", "NOC8", "COM128", "COM256", "COM512"]:
+            for vk in (("f64", "f32") if f in ("COM128", "NOC1", "CSR") else ("f64",)):
+                fo, _ = build_format(F, csr, wl["x"], f)
+                p = D.Plan(csr, fo, val=vk)
+                del fo
+                k = max(20, min(a.steps, 400))
+                s_, _ = timed(lambda: p.spmv(x, y), k, 5, ws, stream, dev)
+                t = s_ / k
+                bb = alg_bytes(n, nnz, 8 if vk == "f64" else 4)
+                formats[f"{p.info['name']}/{vk}"] = {"ms": t * 1e3, "gflops": flops / t / 1e9,
+                                                     "gbs": bb / t / 1e9, "frac": bb / t / 1e9 / peak}
+                del p
+        f64 = formats.get("AXT_COM_BS128/f64")
+        f32 = formats.get("AXT_COM_BS128/f32")
+        if f64 and f32:
+            formats["_fp32_speedup_COM128"] = f64["ms"] / f32["ms"]
+
+    cpu = None
+    if rank == 0 and ws == 1 and not a.no_cpu:
+        try:
+            from oracle import Reference
+            if Reference.available():
+                et, snnz, info = reference_time(wl["row"], wl["col"], wl["val"], wl["x"], a.format, a.cpu_budget)
+                cpu = {"value": 2.0 * snnz / et / 1e9, "unit": UNIT, "cores": info["cores"], "kind": "reference",
+                       "sample": f"{info['kernel']} (intSpmv_main.c) on the full workload, {info['calls']} calls, "
+                                 f"{info['cores']} OpenMP threads; x is baked into ax by the reference builder"}
+            else:
+                cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                       "sample": "unavailable: oracle/_ref missing or host lacks AVX-512"}
+        except Exception as e:  # the baseline must not sink the run
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps, "warmup": W,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": f"synthetic: {wl['desc']} (int_spmv_b200/matrices.py)",
+            "config": {"workload": wl["name"], "format": fmt_name, "n": n, "nnz": nnz,
+                       "value_kind": "FP64 values, FP64 accumulate, u32 columns",
+                       "l2": "no flush: inputs larger than L2 (%.0f MB algorithmic bytes per step)" % (B / 1e6),
+                       "parallelism": f"replicas x{ws} (one full matrix per GPU, no collective)"},
+            "gb_per_s": gbs,
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                         "traffic": traffic_for(f"{wl['name']}/{a.format}"),
+                         "peak_source": peak_src,
+                         "note": "algorithmic bytes nnz*12 + n*20 + 4 over the whole SpMV step "
+                                 "(main kernel + row fix-up launch)"},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": int(round(per_step * a.steps)),
+            "clocks": clocks,
+            "parity": check,
+            "formats": formats,
+        }
+        print(json.dumps(out), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main_reference(a, rank, ws, W):
+    """The reference's own CPU path on the host cores (rank 0 only)."""
+    if rank != 0:
+        return
+    from oracle import Reference
+    if not Reference.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref missing or the host lacks AVX-512"}))
+        return
+    wl = make_workload(a.workload)
+    n, nnz = len(wl["row"]) - 1, len(wl["col"])
+    # size each step so warm-up + timed steps take about two minutes
+    et_full, _, info = reference_time(wl["row"], wl["col"], wl["val"], wl["x"], a.format, 0.0, calls=1)
+    per_step = 120.0 / (a.steps + W)
+    frac = float(min(1.0, max(1.0 / 64, per_step / max(et_full, 1e-9))))
+    et, snnz, info = reference_time(wl["row"], wl["col"], wl["val"], wl["x"], a.format, 0.0,
+                                    calls=a.steps, row_frac=frac, warm=W)
+    value = 2.0 * snnz / et / 1e9
+    fmt_name = {"CSR": "CSR"}.get(a.format, a.format)
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps,
+           "warmup": W, "ms_per_step": et * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": f"synthetic: {wl['desc']}",
+           "config": {"workload": wl["name"], "format": fmt_name, "n": n, "nnz": nnz,
+                      "parallelism": "host OpenMP"},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": info["cores"], "kind": "reference",
+                            "sample": f"{info['kernel']} (intSpmv_main.c) on the first {info['rows']} rows "
+                                      f"({snnz} nonzeros) of the workload per step, {info['cores']} threads"},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

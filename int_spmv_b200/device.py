@@ -1,0 +1,170 @@
+"""Device side: the reference's kernels by name on CUDA tensors, and plans.
+
+`int_axc`, `int_k1`, ... run the sm_100a kernels of libintspmv.so on the
+reference's own arrays (x-baked ax included), stream-ordered on the current
+torch stream, with each reference kernel's output contract (AXT kernels
+accumulate into y: zero it first, as the reference's callers do,
+intSpmv_main.c:1421,1492,1591).
+
+`Plan` uploads a format once and computes y = A x (+ beta y) for a fresh x on
+every call (values FP64, or FP32 with FP64 accumulation).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import abi
+from ._lib import check, load
+from .formats import AXC, AXT, CSR, K1
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("expected a CUDA tensor")
+    if not t.is_contiguous():
+        raise ValueError("expected a contiguous tensor")
+    return t.data_ptr()
+
+
+def _stream(stream=None) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+def to_device(a: np.ndarray, device="cuda") -> torch.Tensor:
+    """u32 arrays travel as int32 tensors (same bits); f64 as float64."""
+    if a.dtype == np.uint32:
+        return torch.from_numpy(a.view(np.int32)).to(device)
+    return torch.from_numpy(np.ascontiguousarray(a)).to(device)
+
+
+# --- the reference's kernels on device tensors (intSpmv_main.c line cited) ---
+
+def cf_CSR(row, col, val, x, y, stream=None):  # :382
+    check(load().ispmv_dev_cf_csr(row.numel() - 1, _ptr(row), _ptr(col), _ptr(val), _ptr(x), _ptr(y),
+                                  _stream(stream)), "ispmv_dev_cf_csr")
+
+
+def int_axc(nrows, ax, brp, y, stream=None):  # :711
+    check(load().ispmv_dev_int_axc(nrows, _ptr(ax), _ptr(brp), _ptr(y), _stream(stream)), "ispmv_dev_int_axc")
+
+
+def int_k1(chunkNum, val, col, chp, nmc, vec, res, stream=None):  # :943
+    check(load().ispmv_dev_int_k1(chunkNum, _ptr(val), _ptr(col), _ptr(chp), _ptr(nmc), _ptr(vec), _ptr(res),
+                                  _stream(stream)), "ispmv_dev_int_k1")
+
+
+def orderArrayK1(length, permi, arrDis, arrOrd, stream=None):  # :969
+    check(load().ispmv_dev_order_k1(length, _ptr(permi), _ptr(arrDis), _ptr(arrOrd), _stream(stream)),
+          "ispmv_dev_order_k1")
+
+
+def int_k1p(mask, chunkNum, val, col, chp, nmc, permi, vec, res, stream=None):  # :1026
+    check(load().ispmv_dev_int_k1p(mask, chunkNum, _ptr(val), _ptr(col), _ptr(chp), _ptr(nmc), _ptr(permi),
+                                   _ptr(vec), _ptr(res), _stream(stream)), "ispmv_dev_int_k1p")
+
+
+def int_axt_noc_h1(tileNum, ax, rwp, y, stream=None):  # :1385
+    check(load().ispmv_dev_int_axt_noc_h1(tileNum, _ptr(ax), _ptr(rwp), _ptr(y), _stream(stream)),
+          "ispmv_dev_int_axt_noc_h1")
+
+
+def int_axt_noc(tileNum, tileHeight, ax, rwp, y, stream=None):  # :1443
+    check(load().ispmv_dev_int_axt_noc(tileNum, tileHeight, _ptr(ax), _ptr(rwp), _ptr(y), _stream(stream)),
+          "ispmv_dev_int_axt_noc")
+
+
+def int_axt_com_h1(bn, bs, log, thw, tn, lenAX, lenRWP, ax, rwp, y, stream=None):  # :1517
+    check(load().ispmv_dev_int_axt_com_h1(bn, bs, log, thw, tn, lenAX, lenRWP, _ptr(ax), _ptr(rwp), _ptr(y),
+                                          _stream(stream)), "ispmv_dev_int_axt_com_h1")
+
+
+# --- plans ---
+
+VAL_KINDS = {"f64": abi.VAL_F64, "f32": abi.VAL_F32, "f32lo": abi.VAL_F32_LO16}
+COL_KINDS = {"u32": abi.COL_U32, "d16": abi.COL_D16}
+KERNELS = {"auto": abi.KERNEL_AUTO, "ldg": abi.KERNEL_LDG, "tma": abi.KERNEL_TMA}
+
+
+def plan_opts(val="f64", col="u32", kernel="auto", units_per_warp=0, ctas_per_sm=0, lo_tol=0.0) -> abi.PlanOpts:
+    o = abi.PlanOpts()
+    load().ispmv_plan_opts_default(C.byref(o))
+    o.val_kind, o.col_kind, o.kernel = VAL_KINDS[val], COL_KINDS[col], KERNELS[kernel]
+    o.units_per_warp, o.ctas_per_sm, o.lo_tol = units_per_warp, ctas_per_sm, lo_tol
+    return o
+
+
+class Plan:
+    """A format resident in HBM.  `fmt` is the host format object built by
+    int_spmv_b200.formats (None for CSR); K1 takes `reorder` (True = int_k1p,
+    False = int_k1 then orderArrayK1)."""
+
+    def __init__(self, csr: CSR, fmt: AXC | K1 | AXT | None = None, *, reorder: bool = True, val="f64", col="u32",
+                 kernel="auto", units_per_warp=0, ctas_per_sm=0, lo_tol=0.0, axi: np.ndarray | None = None):
+        lib = load()
+        o = plan_opts(val, col, kernel, units_per_warp, ctas_per_sm, lo_tol)
+        h = C.c_void_p()
+        if fmt is None:
+            check(lib.ispmv_plan_csr(C.byref(csr.c), C.byref(o), C.byref(h)), "ispmv_plan_csr")
+        elif isinstance(fmt, AXC):
+            axi = fmt.cols() if axi is None else axi
+            check(lib.ispmv_plan_axc(C.byref(csr.c), C.byref(fmt.c), axi.ctypes.data_as(abi.P_UIN), C.byref(o),
+                                     C.byref(h)), "ispmv_plan_axc")
+        elif isinstance(fmt, K1):
+            check(lib.ispmv_plan_k1(C.byref(csr.c), C.byref(fmt.c), int(reorder), C.byref(o), C.byref(h)),
+                  "ispmv_plan_k1")
+        elif isinstance(fmt, AXT):
+            axi = fmt.cols() if axi is None else axi
+            check(lib.ispmv_plan_axt(C.byref(csr.c), C.byref(fmt.c), axi.ctypes.data_as(abi.P_UIN), C.byref(o),
+                                     C.byref(h)), "ispmv_plan_axt")
+        else:
+            raise TypeError(f"unsupported format {type(fmt)}")
+        self._h = h
+        self.n = csr.n
+        self.nnz = csr.nnz
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                load().ispmv_plan_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    @property
+    def info(self) -> dict:
+        i = abi.PlanInfo()
+        check(load().ispmv_plan_get_info(self._h, C.byref(i)), "ispmv_plan_get_info")
+        return dict(nrows=i.nrows, nnz=i.nnz, slots=i.slots, device_bytes=i.device_bytes, alg_bytes=i.alg_bytes,
+                    format=i.format, val_kind=i.val_kind, col_kind=i.col_kind, kernel=i.kernel, tile_h=i.tile_h,
+                    bs=i.bs, name=i.name.decode())
+
+    def spmv(self, x: torch.Tensor, y: torch.Tensor | None = None, beta: int = 0, stream=None) -> torch.Tensor:
+        if x.dtype != torch.float64 or x.numel() != self.n:
+            raise ValueError("x must be a float64 CUDA tensor of n entries")
+        if y is None:
+            y = torch.empty(self.n, dtype=torch.float64, device=x.device)
+        check(load().ispmv_plan_spmv(self._h, _ptr(x), _ptr(y), int(beta), _stream(stream)), "ispmv_plan_spmv")
+        return y
+
+    def spmm(self, X: torch.Tensor, Y: torch.Tensor | None = None, stream=None) -> torch.Tensor:
+        if X.dtype != torch.float64 or X.dim() != 2 or X.shape[0] != self.n:
+            raise ValueError("X must be a float64 CUDA tensor of shape (n, k)")
+        k = X.shape[1]
+        if Y is None:
+            Y = torch.empty((self.n, k), dtype=torch.float64, device=X.device)
+        check(load().ispmv_plan_spmm(self._h, k, _ptr(X), _ptr(Y), _stream(stream)), "ispmv_plan_spmm")
+        return Y
+
+    def spmv_host(self, x: np.ndarray | torch.Tensor, y: np.ndarray | torch.Tensor, stream=None) -> None:
+        """End to end on host buffers (pinned host tensors for full PCIe
+        bandwidth): copy x in, SpMV, copy y out, synchronise."""
+        xp = x.data_ptr() if isinstance(x, torch.Tensor) else x.ctypes.data
+        yp = y.data_ptr() if isinstance(y, torch.Tensor) else y.ctypes.data
+        check(load().ispmv_plan_spmv_host(self._h, xp, yp, _stream(stream)), "ispmv_plan_spmv_host")

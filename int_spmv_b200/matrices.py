@@ -89,45 +89,52 @@ def powerlaw(n: int, seed: int = 1, mu: float = 2.2, sigma: float = 1.0, rl_min:
     """Power-law (lognormal) row lengths: rl = clip(rint(lognormal(mu,
     sigma)), rl_min, rl_max).  Of each row's rl columns, rint(band_frac*rl)
     are uniform in the window [r-band, r+band] clipped to [0, n) and the rest
-    uniform over [0, n); duplicates are redrawn from the same distribution
-    until each row has rl distinct columns.  Values N(0,1).  numpy
-    default_rng(seed) drives everything, in this order: row lengths, then
-    per round band columns, uniform columns; values last."""
+    uniform over [0, n); a column drawn twice in a row is kept once (a band
+    draw before a uniform one) and the lost draw is redrawn from its own
+    distribution until every row has rl distinct columns.  Values N(0,1).
+    numpy default_rng(seed) drives everything, in this order: row lengths,
+    then per round the band columns and the uniform columns; values last."""
     rng = np.random.default_rng(seed)
     rl = np.clip(np.rint(rng.lognormal(mu, sigma, n)), rl_min, min(rl_max, n)).astype(np.int64)
-    nb = np.rint(band_frac * rl).astype(np.int64)
-    nb = np.minimum(nb, np.minimum(np.arange(n) + band, n - 1) - np.maximum(np.arange(n) - band, 0) + 1)
-    need_b, need_r = nb.copy(), rl - nb
-    keys = np.empty(0, dtype=np.int64)
-    r_idx = np.arange(n, dtype=np.int64)
+    r_all = np.arange(n, dtype=np.int64)
+    win = np.minimum(r_all + band, n - 1) - np.maximum(r_all - band, 0) + 1
+    nb = np.minimum(np.rint(band_frac * rl).astype(np.int64), win)
+    need_b, need_r = nb, rl - nb
+    accepted = None  # sorted int64 keys row*n + col
+    extra = np.empty(0, np.int64)
     for _ in range(64):
-        if need_b.sum() == 0 and need_r.sum() == 0:
+        if not need_b.any() and not need_r.any():
             break
-        rb = np.repeat(r_idx, need_b)
+        rb = np.repeat(r_all, need_b)
         lo = np.maximum(rb - band, 0)
-        hi = np.minimum(rb + band, n - 1)
-        cb = lo + (rng.random(rb.size) * (hi - lo + 1)).astype(np.int64)
-        rr = np.repeat(r_idx, need_r)
+        cb = lo + (rng.random(rb.size) * (np.minimum(rb + band, n - 1) - lo + 1)).astype(np.int64)
+        rr = np.repeat(r_all, need_r)
         cr = rng.integers(0, n, rr.size, dtype=np.int64)
-        new_keys = np.concatenate([rb * n + cb, rr * n + cr])
-        new_band = np.concatenate([np.ones(rb.size, bool), np.zeros(rr.size, bool)])
-        # keep existing keys; among new ones keep the first of each duplicate
-        allk = np.concatenate([keys, new_keys])
-        old = np.concatenate([np.ones(keys.size, bool), np.zeros(new_keys.size, bool)])
-        order = np.lexsort((~old, allk))  # by key, existing first
-        sk = allk[order]
-        first = np.ones(sk.size, bool)
-        first[1:] = sk[1:] != sk[:-1]
-        keep = order[first]
-        keep_new = keep[~old[keep]] - keys.size
-        got_rows = new_keys[keep_new] // n
-        got_b = np.bincount(got_rows[new_band[keep_new]], minlength=n)
-        got_r = np.bincount(got_rows[~new_band[keep_new]], minlength=n)
-        need_b -= got_b
-        need_r -= got_r
-        keys = np.sort(allk[keep])
+        # low bit = draw kind (0 band, 1 uniform): sorting keeps a band draw first
+        cand = np.concatenate([(rb * n + cb) << 1, ((rr * n + cr) << 1) | 1])
+        cand.sort()
+        key = cand >> 1
+        first = np.ones(key.size, bool)
+        first[1:] = key[1:] != key[:-1]
+        if accepted is not None:
+            pos = np.searchsorted(accepted, key)
+            hit = (pos < accepted.size) & (accepted[np.minimum(pos, accepted.size - 1)] == key)
+            if extra.size:
+                pe = np.searchsorted(extra, key)
+                hit |= (pe < extra.size) & (extra[np.minimum(pe, extra.size - 1)] == key)
+            first &= ~hit
+        got = key[first]
+        kind = (cand[first] & 1).astype(bool)
+        rows_got = got // n
+        need_b = need_b - np.bincount(rows_got[~kind], minlength=n)
+        need_r = need_r - np.bincount(rows_got[kind], minlength=n)
+        if accepted is None:
+            accepted = got
+        else:
+            extra = np.sort(np.concatenate([extra, got]))
     else:
         raise RuntimeError("power-law generator did not converge")
+    keys = accepted if not extra.size else np.insert(accepted, np.searchsorted(accepted, extra), extra)
     vals = rng.standard_normal(keys.size)
     return _csr_from_sorted_keys(n, keys, vals)
 
@@ -139,7 +146,6 @@ def fem_banded(n: int, rng: np.random.Generator, rl_lo: int = 7, rl_hi: int = 81
     diagonal set to |row sum of the off-diagonals| + 1."""
     rl = rng.integers(rl_lo, rl_hi + 1, n)
     rl = np.minimum(rl, n)
-    rows, cols = [], []
     r_idx = np.arange(n, dtype=np.int64)
     need = rl - 1
     keys = r_idx * n + r_idx  # diagonals
@@ -160,7 +166,6 @@ def fem_banded(n: int, rng: np.random.Generator, rl_lo: int = 7, rl_hi: int = 81
             raise RuntimeError("fem_banded overfilled a row")
     else:
         raise RuntimeError("fem_banded did not converge")
-    del rows, cols
     row, col, _ = _csr_from_sorted_keys(n, keys, np.zeros(keys.size))
     val = rng.standard_normal(keys.size)
     is_diag = (keys // n) == (keys % n)
