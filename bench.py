@@ -44,6 +44,14 @@ def make_workload(name: str):
         return dict(name="powerlaw_n4M_seed1", row=row, col=col, val=val, x=M.uniform_x(4_000_000, 1),
                     desc="power-law n=4,000,000, rl=clip(rint(lognormal(2.2,1.0)),1,5000), 70% band +/-1000, "
                          "30% uniform, N(0,1) values, x~U[-1,1], seed 1")
+    if name == "powerlaw1m":
+        row, col, val = M.powerlaw(1_000_000, seed=3)
+        return dict(name="powerlaw_n1M_seed3", row=row, col=col, val=val, x=M.uniform_x(1_000_000, 3),
+                    desc="power-law n=1,000,000 (same generator, seed 3)")
+    if name == "stencil100":
+        row, col, val = M.stencil27(100, seed=2)
+        return dict(name="stencil27_100", row=row, col=col, val=val, x=M.uniform_x(100 ** 3, 2),
+                    desc="3D 27-point stencil 100^3 (same generator, seed 2)")
     if name == "poisson512":
         row, col, val = M.poisson2d(512)
         return dict(name="poisson2d_512", row=row, col=col, val=val, x=M.uniform_x(512 * 512, 0),
@@ -238,6 +246,7 @@ def main(argv=None):
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="powerlaw4m")
     ap.add_argument("--format", default="COM128")
+    ap.add_argument("--kernel", default="auto", choices=["auto", "ldg", "tma"])
     ap.add_argument("--no-formats", action="store_true", help="skip the per-format table")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of reference CPU work")
@@ -263,7 +272,7 @@ def main(argv=None):
     csr = F.CSR(wl["row"], wl["col"], wl["val"])
     n, nnz = csr.n, csr.nnz
     fmt_obj, fmt_name = build_format(F, csr, wl["x"], a.format)
-    plan = D.Plan(csr, fmt_obj)
+    plan = D.Plan(csr, fmt_obj, kernel=a.kernel)
     del fmt_obj
     stream = torch.cuda.current_stream()
     x = torch.from_numpy(wl["x"]).to(dev)
@@ -312,20 +321,24 @@ def main(argv=None):
 
     formats = {}
     if not a.no_formats:
-        for f in ["CSR", "AXC", "K1", "K1P", "NOC1", "NOC4", "NOC8", "COM128", "COM256", "COM512"]:
-            for vk in (("f64", "f32") if f in ("COM128", "NOC1", "CSR") else ("f64",)):
-                fo, _ = build_format(F, csr, wl["x"], f)
-                p = D.Plan(csr, fo, val=vk)
-                del fo
-                k = max(20, min(a.steps, 400))
-                s_, _ = timed(lambda: p.spmv(x, y), k, 5, ws, stream, dev)
-                t = s_ / k
-                bb = alg_bytes(n, nnz, 8 if vk == "f64" else 4)
-                formats[f"{p.info['name']}/{vk}"] = {"ms": t * 1e3, "gflops": flops / t / 1e9,
-                                                     "gbs": bb / t / 1e9, "frac": bb / t / 1e9 / peak}
-                del p
-        f64 = formats.get("AXT_COM_BS128/f64")
-        f32 = formats.get("AXT_COM_BS128/f32")
+        variants = [(f, "f64", "auto") for f in ["CSR", "AXC", "K1", "K1P", "NOC1", "NOC4", "NOC8", "NOC16",
+                                                    "COM128", "COM256", "COM512"]]
+        variants += [("COM128", "f32", "auto"), ("NOC1", "f32", "auto"), ("CSR", "f32", "auto"),
+                     ("COM128", "f64", "ldg"), ("NOC1", "f64", "ldg"), ("NOC4", "f64", "ldg")]
+        for f, vk, kern in variants:
+            fo, _ = build_format(F, csr, wl["x"], f)
+            p = D.Plan(csr, fo, val=vk, kernel=kern)
+            del fo
+            k = max(20, min(a.steps, 400))
+            s_, _ = timed(lambda: p.spmv(x, y), k, 5, ws, stream, dev)
+            t = s_ / k
+            bb = alg_bytes(n, nnz, 8 if vk == "f64" else 4)
+            kname = {0: "auto", 1: "ldg", 2: "tma"}[p.info["kernel"]]
+            formats[f"{p.info['name']}/{vk}/{kname}"] = {"ms": t * 1e3, "gflops": flops / t / 1e9,
+                                                         "gbs": bb / t / 1e9, "frac": bb / t / 1e9 / peak}
+            del p
+        f64 = formats.get("AXT_COM_BS128/f64/tma")
+        f32 = formats.get("AXT_COM_BS128/f32/tma")
         if f64 and f32:
             formats["_fp32_speedup_COM128"] = f64["ms"] / f32["ms"]
 

@@ -233,9 +233,10 @@ typedef struct ispmv_plan_s *ispmv_plan;
 #define ISPMV_COL_D16 1      /* 16-bit deltas from a per-unit base column */
 
 /* Kernel variants a plan can run (ispmv_plan_opts.kernel). */
-#define ISPMV_KERNEL_AUTO 0
-#define ISPMV_KERNEL_LDG 1   /* register-streaming loads */
-#define ISPMV_KERNEL_TMA 2   /* 1D bulk copies (cp.async.bulk) into shared memory */
+#define ISPMV_KERNEL_AUTO 0  /* the format's default */
+#define ISPMV_KERNEL_LDG 1   /* slot-stream kernel, plain loads, register prefetch */
+#define ISPMV_KERNEL_TMA 2   /* slot-stream kernel, 1D bulk copies (cp.async.bulk) into shared memory */
+#define ISPMV_KERNEL_ROWS 3  /* row-parallel kernel (CSR: lanes per row; AXC: 8 lanes per row; K1) */
 
 typedef struct {
   int val_kind;      /* ISPMV_VAL_* */
@@ -245,6 +246,7 @@ typedef struct {
   int units_per_warp;/* work granule of one warp; 0 = library default */
   double lo_tol;     /* F32_LO16: rows whose FP32 rounding error bound exceeds
                         lo_tol relative carry a lo-word; 0 = default 1e-9 */
+  int variant;       /* kernel variant (prefetch depth / register budget); 0 = default */
 } ispmv_plan_opts;
 
 void ispmv_plan_opts_default(ispmv_plan_opts *o);
@@ -269,6 +271,11 @@ int ispmv_plan_spmm(ispmv_plan p, UIN k, const FPT *X, FPT *Y, void *stream);
 /* End to end on HOST buffers: copies x in, runs the SpMV, copies y out and
  * synchronises `stream`.  Pinned host buffers give full PCIe bandwidth. */
 int ispmv_plan_spmv_host(ispmv_plan p, const FPT *h_x, FPT *h_y, void *stream);
+
+/* Status of the plan's last device work: ISPMV_ERR_TIMEOUT when a bounded
+ * wait of a staged kernel gave up (the result is then invalid), else OK.
+ * Synchronous (reads a device status word). */
+int ispmv_plan_status(ispmv_plan p);
 
 /* Plan facts: rows, nonzeros, value slots streamed, bytes of device
  * storage, and the algorithmic bytes of one SpMV:

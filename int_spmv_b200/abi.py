@@ -49,7 +49,7 @@ class StrMatAXT(C.Structure):  # intSpmv_main.c:1114
 
 class PlanOpts(C.Structure):
     _fields_ = [("val_kind", C.c_int), ("col_kind", C.c_int), ("kernel", C.c_int), ("ctas_per_sm", C.c_int),
-                ("units_per_warp", C.c_int), ("lo_tol", C.c_double)]
+                ("units_per_warp", C.c_int), ("lo_tol", C.c_double), ("variant", C.c_int)]
 
 
 class PlanInfo(C.Structure):
@@ -119,6 +119,7 @@ PROTOTYPES: dict[str, tuple] = {
     "ispmv_plan_spmm": (C.c_int, [VP, UIN, VP, VP, VP]),
     "ispmv_plan_spmv_host": (C.c_int, [VP, VP, VP, VP]),
     "ispmv_plan_get_info": (C.c_int, [VP, C.POINTER(PlanInfo)]),
+    "ispmv_plan_status": (C.c_int, [VP]),
     # library facts
     "ispmv_version": (C.c_char_p, []),
     "ispmv_status_string": (C.c_char_p, [C.c_int]),
@@ -130,4 +131,4 @@ PROTOTYPES: dict[str, tuple] = {
 OK, ERR_ARG, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_OVERFLOW = range(7)
 VAL_F64, VAL_F32, VAL_F32_LO16 = 0, 1, 2
 COL_U32, COL_D16 = 0, 1
-KERNEL_AUTO, KERNEL_LDG, KERNEL_TMA = 0, 1, 2
+KERNEL_AUTO, KERNEL_LDG, KERNEL_TMA, KERNEL_ROWS = 0, 1, 2, 3

@@ -2,35 +2,41 @@
 // column-index stream plus the format's row structure, then y = A*x +
 // beta*y for a fresh x on every call.
 //
-// Device layouts (all slot streams in the reference format's own slot
-// order, x halves of `ax` dropped and replaced by the column companion):
-//   CSR      val[nnz], col[nnz], row[n+1]                    (csr_vec)
-//   AXC      val/col[lenAX/2] in brick order, brick row pointer brp/16
-//   K1       val/col[lenVC] column-major per chunk, chp, nmc, permi
-//   AXT NOC  val/col[lenAX/2] in tile order, sec cut to the used units
-//   AXT COM  val/col[nnz] (packed = CSR order), a row-start bitmap (1 bit
-//            per slot) and a per-segment start count instead of the
-//            reference's 4-byte-per-slot descriptors, plus the compressed ->
-//            real row map when some rows are empty.
+// Device layouts (slot streams in the reference format's own slot order; the
+// x halves of `ax` are dropped and the column companion takes their place):
+//   stream  CSR / AXT COM (CSR order), AXT NOC tileH=1 (tile order, rows
+//           padded to 8) and AXC (brick order, rows padded to 8): val[S],
+//           col[S] zero-padded to a multiple of 512 slots, a row-start bitmap
+//           (1 bit per slot), per-segment start counts, and the compressed ->
+//           real row map when some rows are empty.  Kernels: sss::stream_ldg,
+//           sss::stream_tma.
+//   units   AXT NOC tileH>1 (tile columns): val/col in tile order plus the
+//           reference's per-column row array (sec) cut to the used columns.
+//           Kernels: pk::noc_hn, tk::nocn_tma.
+//   rows    CSR row pointer (pk::csr_vec) and AXC brick pointer
+//           (pk::axc_rows): the row-parallel kernels.
+//   K1      val/col column-major per chunk, chp, nmc, permi (pk::k1_chunks).
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
 #include <vector>
 
-#include "plan_kernels.cuh"
+#include "plan_tma.cuh"
+#include "sss.cuh"
 
 using namespace ispmv;
 
 enum PlanFormat { F_CSR = 0, F_AXC = 1, F_K1 = 2, F_K1P = 3, F_AXT_NOC = 4, F_AXT_COM = 5 };
+enum PlanPath { P_STREAM = 0, P_UNITS = 1, P_ROWS = 2, P_K1 = 3 };
 
 struct ispmv_plan_s {
   int fmt = 0;
+  int path = P_STREAM;
   ispmv_plan_opts opts{};
-  int device = 0;
   UIN n = 0, nnz = 0, th = 1, bs = 0, lanes = 8;
-  size_t slots = 0, nunits = 0;
+  size_t slots = 0, slots_pad = 0, nunits = 0;
+  size_t seg_slots = 0, nseg = 0;
   UIN useg = 0;
-  size_t nseg = 0;
   void *val = nullptr;  // double or float
   UIN *col = nullptr;
   UIN *rows = nullptr;  // row / brick pointer, or unit rows
@@ -41,12 +47,22 @@ struct ispmv_plan_s {
   FPT *res = nullptr;  // K1 result in chunk order
   UIN *rec_row = nullptr;
   double *rec_sum = nullptr;
+  int *status = nullptr;
   FPT *hx = nullptr, *hy = nullptr;  // device staging of ispmv_plan_spmv_host
   std::vector<void *> owned;
   ispmv_plan_info info{};
 };
 
 namespace {
+
+constexpr size_t SS = sss::SS;      // slots per staged stage; streams pad to it
+constexpr size_t SEG_SLOTS = 2048;  // default slots per warp segment
+
+#define TRY(expr)        \
+  do {                   \
+    int s__ = (expr);    \
+    if (s__) return s__; \
+  } while (0)
 
 template <typename T>
 int dev_upload(ispmv_plan_s *p, const T *h, size_t n, T **d) {
@@ -62,30 +78,22 @@ int dev_alloc(ispmv_plan_s *p, size_t n, T **d) {
   return dev_upload<T>(p, nullptr, n, d);
 }
 
-#define TRY(expr)           \
-  do {                      \
-    int s__ = (expr);       \
-    if (s__) return s__;    \
-  } while (0)
+size_t vbytes(const ispmv_plan_s *p) { return p->opts.val_kind == ISPMV_VAL_F64 ? 8 : 4; }
 
 int upload_values(ispmv_plan_s *p, const std::vector<double> &v) {
   if (p->opts.val_kind == ISPMV_VAL_F64) {
     double *d;
     TRY(dev_upload(p, v.data(), v.size(), &d));
     p->val = d;
-  } else if (p->opts.val_kind == ISPMV_VAL_F32) {
-    std::vector<float> f(v.size());
-    for (size_t i = 0; i < v.size(); i++) f[i] = (float)v[i];
-    float *d;
-    TRY(dev_upload(p, f.data(), f.size(), &d));
-    p->val = d;
-  } else {
-    return ISPMV_ERR_UNSUPPORTED;
+    return ISPMV_OK;
   }
+  std::vector<float> f(v.size());
+  for (size_t i = 0; i < v.size(); i++) f[i] = (float)v[i];
+  float *d;
+  TRY(dev_upload(p, f.data(), f.size(), &d));
+  p->val = d;
   return ISPMV_OK;
 }
-
-size_t vbytes(const ispmv_plan_s *p) { return p->opts.val_kind == ISPMV_VAL_F64 ? 8 : 4; }
 
 void finish_info(ispmv_plan_s *p, const char *name) {
   ispmv_plan_info &i = p->info;
@@ -103,30 +111,6 @@ void finish_info(ispmv_plan_s *p, const char *name) {
   snprintf(i.name, sizeof i.name, "%s", name);
 }
 
-// segment sizes: about 2048 slots per warp, a multiple of 32 units
-UIN pick_useg(ispmv_plan_s *p, UIN slots_per_unit) {
-  UIN u = p->opts.units_per_warp;
-  if (!u) u = std::max<UIN>(32u, (2048u / std::max<UIN>(1u, slots_per_unit)) & ~31u);
-  u = std::max<UIN>(32u, u & ~31u);
-  return u;
-}
-
-int alloc_records(ispmv_plan_s *p) {
-  p->nseg = (p->nunits + p->useg - 1) / p->useg;
-  TRY(dev_alloc(p, std::max<size_t>(1, 2 * p->nseg), &p->rec_row));
-  TRY(dev_alloc(p, std::max<size_t>(1, 2 * p->nseg), &p->rec_sum));
-  return ISPMV_OK;
-}
-
-int empty_rows(ispmv_plan_s *p, const str_matCSR *csr) {
-  std::vector<UIN> e;
-  for (UIN r = 0; r < csr->nrows; r++)
-    if (csr->row[r + 1] == csr->row[r]) e.push_back(r);
-  p->nempty = e.size();
-  if (!e.empty()) TRY(dev_upload(p, e.data(), e.size(), &p->empty));
-  return ISPMV_OK;
-}
-
 int check_csr(const str_matCSR *csr) {
   if (!csr || !csr->row || csr->nrows == 0) return ISPMV_ERR_ARG;
   if (csr->nnz && (!csr->col || !csr->val)) return ISPMV_ERR_ARG;
@@ -141,15 +125,11 @@ int begin(const ispmv_plan_opts *o, ispmv_plan_s **out) {
   if (!p) return ISPMV_ERR_OOM;
   if (o) p->opts = *o;
   else ispmv_plan_opts_default(&p->opts);
-  if (p->opts.val_kind != ISPMV_VAL_F64 && p->opts.val_kind != ISPMV_VAL_F32) {
+  if ((p->opts.val_kind != ISPMV_VAL_F64 && p->opts.val_kind != ISPMV_VAL_F32) || p->opts.col_kind != ISPMV_COL_U32 ||
+      p->opts.kernel < 0 || p->opts.kernel > ISPMV_KERNEL_ROWS) {
     delete p;
     return ISPMV_ERR_UNSUPPORTED;
   }
-  if (p->opts.col_kind != ISPMV_COL_U32) {
-    delete p;
-    return ISPMV_ERR_UNSUPPORTED;
-  }
-  cudaGetDevice(&p->device);
   *out = p;
   return ISPMV_OK;
 }
@@ -160,6 +140,67 @@ int done(ispmv_plan_s *p, int st, ispmv_plan *out) {
     return st;
   }
   *out = p;
+  return ISPMV_OK;
+}
+
+int empty_rows(ispmv_plan_s *p, const str_matCSR *csr) {
+  std::vector<UIN> e;
+  for (UIN r = 0; r < csr->nrows; r++)
+    if (csr->row[r + 1] == csr->row[r]) e.push_back(r);
+  p->nempty = e.size();
+  if (!e.empty()) TRY(dev_upload(p, e.data(), e.size(), &p->empty));
+  return ISPMV_OK;
+}
+
+int alloc_records(ispmv_plan_s *p) {
+  TRY(dev_alloc(p, std::max<size_t>(1, 2 * p->nseg), &p->rec_row));
+  TRY(dev_alloc(p, std::max<size_t>(1, 2 * p->nseg), &p->rec_sum));
+  TRY(dev_alloc(p, 1, &p->status));
+  ISPMV_TRY(cudaMemset(p->status, 0, sizeof(int)));
+  return ISPMV_OK;
+}
+
+size_t seg_slots_of(const ispmv_plan_s *p, size_t upu) {
+  if (p->opts.units_per_warp <= 0) return SEG_SLOTS;
+  return std::max(SS, ((size_t)p->opts.units_per_warp * upu + SS - 1) / SS * SS);
+}
+
+// The stream path: `v`/`c` the slot streams (length p->slots), `start[r]`
+// the first slot of row r (rows with no slot are skipped).
+int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v, std::vector<UIN> &c,
+                 const std::vector<size_t> &start) {
+  p->path = P_STREAM;
+  p->slots_pad = std::max(SS, (p->slots + SS - 1) / SS * SS);
+  v.resize(p->slots_pad, 0.0);
+  c.resize(p->slots_pad, 0);
+  TRY(upload_values(p, v));
+  TRY(dev_upload(p, c.data(), c.size(), &p->col));
+  std::vector<UIN> heads(p->slots_pad / 32, 0), rowmap;
+  bool any_empty = false;
+  for (UIN r = 0; r < p->n; r++) {
+    if (csr->row[r + 1] == csr->row[r]) {
+      any_empty = true;
+      continue;
+    }
+    const size_t q = start[r];
+    heads[q >> 5] |= 1u << (q & 31);
+    rowmap.push_back(r);
+  }
+  p->seg_slots = seg_slots_of(p, 1);
+  p->nseg = (p->slots_pad + p->seg_slots - 1) / p->seg_slots;
+  std::vector<UIN> segh(std::max<size_t>(1, p->nseg), 0);
+  UIN acc = 0;
+  for (size_t sg = 0, w = 0; sg < p->nseg; sg++) {
+    const size_t wend = std::min(heads.size(), (sg * p->seg_slots) >> 5);
+    for (; w < wend; w++) acc += __builtin_popcount(heads[w]);
+    segh[sg] = acc;
+  }
+  TRY(dev_upload(p, heads.data(), heads.size(), &p->heads));
+  TRY(dev_upload(p, segh.data(), segh.size(), &p->segh));
+  if (any_empty) TRY(dev_upload(p, rowmap.data(), rowmap.size(), &p->rowmap));
+  TRY(empty_rows(p, csr));
+  TRY(alloc_records(p));
+  p->info.device_bytes = (uint64_t)p->slots_pad * (vbytes(p) + 4) + p->slots_pad / 8;
   return ISPMV_OK;
 }
 
@@ -189,14 +230,25 @@ ISPMV_API int ispmv_plan_csr(const str_matCSR *csr, const ispmv_plan_opts *o, is
   p->n = csr->nrows;
   p->nnz = csr->nnz;
   p->slots = csr->nnz;
-  const double mean = (double)csr->nnz / csr->nrows;
-  p->lanes = mean <= 2.5 ? 2 : mean <= 5 ? 4 : mean <= 12 ? 8 : mean <= 24 ? 16 : 32;
-  std::vector<double> v(csr->val, csr->val + csr->nnz);
-  int st = upload_values(p, v);
-  if (!st) st = dev_upload(p, csr->col, csr->nnz, &p->col);
-  if (!st) st = dev_upload(p, csr->row, (size_t)csr->nrows + 1, &p->rows);
+  int st = ISPMV_OK;
+  if (p->opts.kernel == ISPMV_KERNEL_AUTO || p->opts.kernel == ISPMV_KERNEL_ROWS) {
+    // the naive CSR product on the GPU: L lanes per row
+    p->opts.kernel = ISPMV_KERNEL_ROWS;
+    p->path = P_ROWS;
+    const double mean = (double)csr->nnz / csr->nrows;
+    p->lanes = mean <= 2.5 ? 2 : mean <= 5 ? 4 : mean <= 12 ? 8 : mean <= 24 ? 16 : 32;
+    std::vector<double> v(csr->val, csr->val + csr->nnz);
+    st = upload_values(p, v);
+    if (!st) st = dev_upload(p, csr->col, csr->nnz, &p->col);
+    if (!st) st = dev_upload(p, csr->row, (size_t)csr->nrows + 1, &p->rows);
+    p->info.device_bytes = (uint64_t)csr->nnz * (vbytes(p) + 4) + 4ull * (csr->nrows + 1);
+  } else {
+    std::vector<double> v(csr->val, csr->val + csr->nnz);
+    std::vector<UIN> c(csr->col, csr->col + csr->nnz);
+    std::vector<size_t> start(csr->row, csr->row + csr->nrows);
+    st = setup_stream(p, csr, v, c, start);
+  }
   finish_info(p, "CSR");
-  p->info.device_bytes = (uint64_t)csr->nnz * (vbytes(p) + 4) + 4ull * (csr->nrows + 1);
   return done(p, st, out);
 }
 
@@ -212,14 +264,25 @@ ISPMV_API int ispmv_plan_axc(const str_matCSR *csr, const str_matAXC *axc, const
   p->nnz = csr->nnz;
   p->slots = axc->lenAX / 2;
   std::vector<double> v(p->slots);
+  std::vector<UIN> c(axi, axi + p->slots);
   for (size_t s = 0; s < p->slots; s++) v[s] = axc->ax[(s / 8) * 16 + s % 8];
-  std::vector<UIN> bptr((size_t)p->n + 1);
-  for (size_t r = 0; r <= p->n; r++) bptr[r] = axc->brp[r] / 16;
-  int st = upload_values(p, v);
-  if (!st) st = dev_upload(p, axi, p->slots, &p->col);
-  if (!st) st = dev_upload(p, bptr.data(), bptr.size(), &p->rows);
+  int st = ISPMV_OK;
+  if (p->opts.kernel == ISPMV_KERNEL_AUTO || p->opts.kernel == ISPMV_KERNEL_ROWS) {
+    // the reference's row loop (M:711-732): 8 lanes per row over its bricks
+    p->opts.kernel = ISPMV_KERNEL_ROWS;
+    p->path = P_ROWS;
+    std::vector<UIN> bptr((size_t)p->n + 1);
+    for (size_t r = 0; r <= p->n; r++) bptr[r] = axc->brp[r] / 16;
+    st = upload_values(p, v);
+    if (!st) st = dev_upload(p, c.data(), c.size(), &p->col);
+    if (!st) st = dev_upload(p, bptr.data(), bptr.size(), &p->rows);
+    p->info.device_bytes = (uint64_t)p->slots * (vbytes(p) + 4) + 4ull * (p->n + 1);
+  } else {
+    std::vector<size_t> start(p->n);
+    for (UIN r = 0; r < p->n; r++) start[r] = axc->brp[r] / 2;
+    st = setup_stream(p, csr, v, c, start);
+  }
   finish_info(p, "AXC");
-  p->info.device_bytes = (uint64_t)p->slots * (vbytes(p) + 4) + 4ull * (p->n + 1);
   return done(p, st, out);
 }
 
@@ -232,6 +295,8 @@ ISPMV_API int ispmv_plan_k1(const str_matCSR *csr, const str_matK1 *k1, int reor
   ispmv_plan_s *p;
   TRY(begin(o, &p));
   p->fmt = reorder ? F_K1P : F_K1;
+  p->path = P_K1;
+  p->opts.kernel = ISPMV_KERNEL_ROWS;
   p->n = csr->nrows;
   p->nnz = csr->nnz;
   p->slots = k1->lenVC;
@@ -252,74 +317,79 @@ ISPMV_API int ispmv_plan_k1(const str_matCSR *csr, const str_matK1 *k1, int reor
 ISPMV_API int ispmv_plan_axt(const str_matCSR *csr, const str_matAXT *axt, const UIN *axi, const ispmv_plan_opts *o,
                              ispmv_plan *out) {
   TRY(check_csr(csr));
-  if (!axt || !axi || !axt->ax || !axt->sec || axt->nrows != csr->nrows) return ISPMV_ERR_ARG;
+  if (!axt || !axi || !axt->ax || !axt->sec || !axt->con || axt->nrows != csr->nrows) return ISPMV_ERR_ARG;
   if (axt->tileHW != 8 || axt->tileH == 0) return ISPMV_ERR_UNSUPPORTED;
   const bool com = std::strncmp(axt->mode, "COM", 3) == 0;
   const bool noc = std::strncmp(axt->mode, "NOC", 3) == 0;
   if (!com && !noc) return ISPMV_ERR_ARG;
+  if (com && axt->tileH != 1) return ISPMV_ERR_UNSUPPORTED;
   ispmv_plan_s *p;
   TRY(begin(o, &p));
+  if (p->opts.kernel == ISPMV_KERNEL_ROWS) {
+    delete p;
+    return ISPMV_ERR_UNSUPPORTED;
+  }
   p->n = csr->nrows;
   p->nnz = csr->nnz;
   p->th = axt->tileH;
-  int st = ISPMV_OK;
+  p->fmt = com ? F_AXT_COM : F_AXT_NOC;
   char name[32];
-  if (noc) {
-    p->fmt = F_AXT_NOC;
-    const UIN th = axt->tileH, grp = th == 1 ? 8 : th;
-    size_t slots = 0;
-    for (UIN r = 0; r < p->n; r++) slots += ((size_t)csr->rl[r] + grp - 1) / grp * grp;
-    p->slots = (size_t)axt->lenAX / 2;
-    p->nunits = th == 1 ? slots / 8 : slots / th;  // used tiles / tile columns
-    std::vector<double> v(p->slots);
-    for (size_t s = 0; s < p->slots; s++) v[s] = axt->ax[(s / 8) * 16 + s % 8];
-    st = upload_values(p, v);
-    if (!st) st = dev_upload(p, axi, p->slots, &p->col);
-    if (!st) st = dev_upload(p, axt->sec, p->nunits, &p->rows);
-    p->useg = pick_useg(p, th == 1 ? 8 : th);
-    snprintf(name, sizeof name, "AXT_NOC_H%u", th);
-  } else {
-    if (axt->tileH != 1) { ispmv_plan_destroy(p); return ISPMV_ERR_UNSUPPORTED; }
-    p->fmt = F_AXT_COM;
+  int st = ISPMV_OK;
+  const UIN th = axt->tileH;
+  if (com) {
     p->bs = 1u << axt->log;
-    p->slots = csr->nnz;
-    p->nunits = csr->nnz;
-    std::vector<double> v(p->slots);
-    std::vector<UIN> c(p->slots);
-    for (size_t s = 0; s < p->slots; s++) {
-      v[s] = axt->ax[(s / 8) * 16 + s % 8];
-      c[s] = axi[s];
-    }
-    st = upload_values(p, v);
-    if (!st) st = dev_upload(p, c.data(), c.size(), &p->col);
-    p->useg = pick_useg(p, 1);
-    // row-start bitmap, per-segment start counts, compressed -> real rows
-    const size_t nw = (p->slots + 31) / 32;
-    std::vector<UIN> heads(std::max<size_t>(1, nw), 0), rowmap;
-    bool any_empty = false;
-    for (UIN r = 0; r < p->n; r++) {
-      if (csr->row[r + 1] == csr->row[r]) { any_empty = true; continue; }
-      const size_t s = csr->row[r];
-      heads[s >> 5] |= 1u << (s & 31);
-      rowmap.push_back(r);
-    }
-    const size_t nseg = (p->nunits + p->useg - 1) / p->useg;
-    std::vector<UIN> segh(std::max<size_t>(1, nseg), 0);
-    UIN acc = 0;
-    for (size_t sg = 0, w = 0; sg < nseg; sg++) {
-      const size_t wend = (sg * p->useg) >> 5;
-      for (; w < wend; w++) acc += __builtin_popcount(heads[w]);
-      segh[sg] = acc;
-    }
-    if (!st) st = dev_upload(p, heads.data(), heads.size(), &p->heads);
-    if (!st) st = dev_upload(p, segh.data(), segh.size(), &p->segh);
-    if (!st && any_empty) st = dev_upload(p, rowmap.data(), rowmap.size(), &p->rowmap);
     snprintf(name, sizeof name, "AXT_COM_BS%u", p->bs);
+  } else {
+    snprintf(name, sizeof name, "AXT_NOC_H%u", th);
   }
-  if (!st) st = empty_rows(p, csr);
-  if (!st) st = alloc_records(p);
+  if (com || th == 1) {
+    // the tileH=1 tile stream and the packed compacted stream: every row is
+    // a contiguous run of slots starting at the slot its con[] names
+    p->slots = com ? csr->nnz : (size_t)axt->lenAX / 2;
+    std::vector<double> v(p->slots);
+    std::vector<UIN> c(axi, axi + p->slots);
+    for (size_t q = 0; q < p->slots; q++) v[q] = axt->ax[(q / 8) * 16 + q % 8];
+    std::vector<size_t> start(p->n);
+    for (UIN r = 0; r < p->n; r++) start[r] = (size_t)(axt->con[r] / 16) * 8 + axt->con[r] % 16;
+    if (p->opts.kernel == ISPMV_KERNEL_AUTO) p->opts.kernel = ISPMV_KERNEL_LDG;
+    st = setup_stream(p, csr, v, c, start);
+  } else {
+    // tile columns: the unit engine on the reference's per-column rows
+    p->path = P_UNITS;
+    size_t used = 0;
+    for (UIN r = 0; r < p->n; r++) used += ((size_t)csr->rl[r] + th - 1) / th * th;
+    p->slots = (size_t)axt->lenAX / 2;
+    p->nunits = used / th;
+    p->slots_pad = std::max(SS, (p->slots + SS - 1) / SS * SS);
+    const bool regular = th == 4 || th == 8 || th == 16;
+    if (p->opts.kernel == ISPMV_KERNEL_TMA && !regular) st = ISPMV_ERR_UNSUPPORTED;
+    if (p->opts.kernel == ISPMV_KERNEL_AUTO) p->opts.kernel = ISPMV_KERNEL_LDG;
+    if (regular) {
+      p->seg_slots = seg_slots_of(p, th);
+      p->useg = (UIN)(p->seg_slots / th);
+      p->nseg = (p->slots_pad + p->seg_slots - 1) / p->seg_slots;
+    } else {
+      UIN u = p->opts.units_per_warp > 0 ? (UIN)p->opts.units_per_warp : std::max<UIN>(32u, (2048u / th) & ~31u);
+      p->useg = std::max<UIN>(32u, u & ~31u);
+      p->seg_slots = (size_t)p->useg * th;
+      p->nseg = (p->nunits + p->useg - 1) / p->useg;
+    }
+    std::vector<double> v(p->slots_pad, 0.0);
+    std::vector<UIN> c(p->slots_pad, 0);
+    for (size_t q = 0; q < p->slots; q++) {
+      v[q] = axt->ax[(q / 8) * 16 + q % 8];
+      c[q] = axi[q];
+    }
+    if (!st) st = upload_values(p, v);
+    if (!st) st = dev_upload(p, c.data(), c.size(), &p->col);
+    std::vector<UIN> ur(std::max<size_t>(p->slots_pad / th, p->nunits) + 32, NO_ROW);
+    std::copy(axt->sec, axt->sec + p->nunits, ur.begin());
+    if (!st) st = dev_upload(p, ur.data(), ur.size(), &p->rows);
+    if (!st) st = empty_rows(p, csr);
+    if (!st) st = alloc_records(p);
+    p->info.device_bytes = (uint64_t)p->slots_pad * (vbytes(p) + 4) + 4ull * p->nunits;
+  }
   finish_info(p, name);
-  p->info.device_bytes = (uint64_t)p->slots * (vbytes(p) + 4);
   return done(p, st, out);
 }
 
@@ -332,11 +402,91 @@ ISPMV_API int ispmv_plan_get_info(ispmv_plan p, ispmv_plan_info *info) {
 // ------------------------------------------------------------ execute --
 namespace {
 
+constexpr int TW = 4;  // warps per CTA of the staged kernels
+constexpr int TS = 4;  // stages per warp
+
+template <typename K>
+int launch_staged(K kernel, size_t smem, size_t nseg, int ctas_per_sm, cudaStream_t s, const char *what,
+                  void **args) {
+  const size_t want = (nseg + TW - 1) / TW;
+  const size_t cap = (size_t)sm_count() * (size_t)(ctas_per_sm > 0 ? ctas_per_sm : 2);
+  const unsigned g = (unsigned)std::max<size_t>(1, std::min(want, cap));
+  ISPMV_TRY(cudaFuncSetAttribute((const void *)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  ISPMV_TRY(cudaLaunchKernel((const void *)kernel, dim3(g), dim3(TW * 32), args, smem, s));
+  return check_launch(what);
+}
+
+template <typename VT>
+int run_stream(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
+  const VT *val = static_cast<const VT *>(p->val);
+  size_t nslots = p->slots, spad = p->slots_pad, sslots = p->seg_slots, nseg = p->nseg;
+  const UIN *col = p->col, *heads = p->heads, *segh = p->segh;
+  if (p->opts.kernel == ISPMV_KERNEL_TMA) {
+    int *status = p->status;
+    void *args[] = {&nslots, &spad, &sslots, &nseg, &val, &col, &heads, &segh, (void *)&x, &o, &status};
+    return launch_staged(sss::stream_tma<VT, TW, TS>, sss::smem_bytes<TW, TS, VT>(), nseg, p->opts.ctas_per_sm, s,
+                         "stream_tma", args);
+  }
+  const unsigned g = (unsigned)((nseg * 32 + 255) / 256);
+  // variants: slots per lane x prefetch depth (batches in flight) x CTAs per
+  // SM the register budget allows; variant 0 is the default
+#define ISPMV_SSS(SPL, PD, MINB)                                                                              \
+  sss::stream_ldg<VT, SPL, PD, MINB><<<g, 256, 0, s>>>(nslots, spad, sslots, nseg, val, col, heads, segh, x, o); \
+  break
+  switch (p->opts.variant) {
+    case 1: ISPMV_SSS(4, 1, 4);
+    case 2: ISPMV_SSS(4, 0, 5);
+    case 3: ISPMV_SSS(2, 1, 6);
+    case 4: ISPMV_SSS(2, 0, 8);
+    case 5: ISPMV_SSS(2, 1, 5);
+    case 6: ISPMV_SSS(4, 0, 8);
+    case 7: ISPMV_SSS(2, 0, 6);
+    default: ISPMV_SSS(4, 0, 6);
+  }
+#undef ISPMV_SSS
+  return check_launch("stream_ldg");
+}
+
+template <typename VT>
+int run_units(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
+  const VT *val = static_cast<const VT *>(p->val);
+  if (p->opts.kernel == ISPMV_KERNEL_TMA) {
+    using L = tk::StageLayout<VT>;
+    size_t nunits = p->nunits, spad = p->slots_pad, nseg = p->nseg, sslots = p->seg_slots;
+    const UIN *col = p->col, *urow = p->rows;
+    int *status = p->status;
+    void *args[] = {&nunits, &spad, &nseg, &sslots, &val, &col, &urow, (void *)&x, &o, &status};
+    const int cps = p->opts.ctas_per_sm;
+    switch (p->th) {
+      case 4:
+        return launch_staged(tk::nocn_tma<VT, 4, TW, TS>, tk::smem_bytes<TW, TS>(L::VB + L::CB + (tk::SS / 4) * 4),
+                             nseg, cps, s, "nocn_tma<4>", args);
+      case 8:
+        return launch_staged(tk::nocn_tma<VT, 8, TW, TS>, tk::smem_bytes<TW, TS>(L::VB + L::CB + (tk::SS / 8) * 4),
+                             nseg, cps, s, "nocn_tma<8>", args);
+      case 16:
+        return launch_staged(tk::nocn_tma<VT, 16, TW, TS>,
+                             tk::smem_bytes<TW, TS>(L::VB + L::CB + (tk::SS / 16) * 4), nseg, cps, s, "nocn_tma<16>",
+                             args);
+      default:
+        return ISPMV_ERR_UNSUPPORTED;
+    }
+  }
+  const unsigned g = (unsigned)((p->nseg * 32 + pk::TPB - 1) / pk::TPB);
+  pk::noc_hn<VT><<<g, pk::TPB, 0, s>>>(p->nunits, p->nseg, p->th, p->useg, p->rows, p->col, val, x, o);
+  return check_launch("noc_hn");
+}
+
 template <typename VT>
 int run(ispmv_plan_s *p, const FPT *x, FPT *y, int beta, cudaStream_t s) {
   const VT *val = static_cast<const VT *>(p->val);
-  switch (p->fmt) {
-    case F_CSR: {
+  switch (p->path) {
+    case P_ROWS: {
+      if (p->fmt == F_AXC) {
+        const unsigned g = (unsigned)(((size_t)p->n * 8 + pk::TPB - 1) / pk::TPB);
+        pk::axc_rows<VT><<<g, pk::TPB, 0, s>>>(p->n, p->rows, p->col, val, x, y, beta);
+        return check_launch("axc_rows");
+      }
       const size_t thr = (size_t)p->n * p->lanes;
       const unsigned g = (unsigned)((thr + pk::TPB - 1) / pk::TPB);
       switch (p->lanes) {
@@ -348,13 +498,7 @@ int run(ispmv_plan_s *p, const FPT *x, FPT *y, int beta, cudaStream_t s) {
       }
       return check_launch("csr_vec");
     }
-    case F_AXC: {
-      const unsigned g = (unsigned)(((size_t)p->n * 8 + pk::TPB - 1) / pk::TPB);
-      pk::axc_rows<VT><<<g, pk::TPB, 0, s>>>(p->n, p->rows, p->col, val, x, y, beta);
-      return check_launch("axc_rows");
-    }
-    case F_K1:
-    case F_K1P: {
+    case P_K1: {
       const unsigned g = (unsigned)(((size_t)p->chunkNum * 8 + pk::TPB - 1) / pk::TPB);
       if (p->fmt == F_K1P) {
         pk::k1_chunks<VT, true><<<g, pk::TPB, 0, s>>>(p->n, p->chunkNum, p->chp, p->nmc, p->permi, p->col, val, x, y,
@@ -363,27 +507,15 @@ int run(ispmv_plan_s *p, const FPT *x, FPT *y, int beta, cudaStream_t s) {
       }
       pk::k1_chunks<VT, false><<<g, pk::TPB, 0, s>>>(p->n, p->chunkNum, p->chp, p->nmc, p->permi, p->col, val, x,
                                                      p->res, beta);
-      int st = check_launch("k1_chunks");
-      if (st) return st;
+      TRY(check_launch("k1_chunks"));
       pk::k1_order<<<(unsigned)((p->n + 255) / 256), 256, 0, s>>>(p->n, p->permi, p->res, y, beta);
       return check_launch("k1_order");
     }
-    case F_AXT_NOC:
-    case F_AXT_COM: {
+    case P_STREAM:
+    case P_UNITS: {
       seg::Out o{y, p->rowmap, p->rec_row, p->rec_sum, beta};
-      if (p->nunits) {
-        const unsigned g = (unsigned)((p->nseg * 32 + pk::TPB - 1) / pk::TPB);
-        if (p->fmt == F_AXT_COM) {
-          pk::com_slots<VT><<<g, pk::TPB, 0, s>>>(p->nunits, p->useg, p->heads, p->segh, p->col, val, x, o);
-        } else if (p->th == 1) {
-          pk::noc_h1<VT><<<g, pk::TPB, 0, s>>>(p->nunits, p->useg, p->rows, p->col, val, x, o);
-        } else {
-          pk::noc_hn<VT><<<g, pk::TPB, 0, s>>>(p->nunits, p->th, p->useg, p->rows, p->col, val, x, o);
-        }
-        int st = check_launch("axt main");
-        if (st) return st;
-      }
-      const size_t nrec = 2 * p->nseg;
+      if (p->slots) TRY(p->path == P_STREAM ? run_stream<VT>(p, x, o, s) : run_units<VT>(p, x, o, s));
+      const size_t nrec = p->slots ? 2 * p->nseg : 0;
       const size_t work = std::max(nrec, p->nempty);
       if (work) {
         seg::fixup<<<(unsigned)((work + 255) / 256), 256, 0, s>>>(nrec, p->rec_row, p->rec_sum, p->rowmap, p->empty,
@@ -406,6 +538,14 @@ ISPMV_API int ispmv_plan_spmv(ispmv_plan p, const FPT *x, FPT *y, int beta, void
   return run<float>(p, x, y, beta, s);
 }
 
+ISPMV_API int ispmv_plan_status(ispmv_plan p) {
+  if (!p) return ISPMV_ERR_ARG;
+  if (!p->status) return ISPMV_OK;
+  int v = 0;
+  ISPMV_TRY(cudaMemcpy(&v, p->status, sizeof v, cudaMemcpyDeviceToHost));
+  return v;
+}
+
 ISPMV_API int ispmv_plan_spmv_host(ispmv_plan p, const FPT *h_x, FPT *h_y, void *stream) {
   if (!p || !h_x || !h_y) return ISPMV_ERR_ARG;
   if (!p->hx) {
@@ -417,7 +557,7 @@ ISPMV_API int ispmv_plan_spmv_host(ispmv_plan p, const FPT *h_x, FPT *h_y, void 
   TRY(ispmv_plan_spmv(p, p->hx, p->hy, 0, stream));
   ISPMV_TRY(cudaMemcpyAsync(h_y, p->hy, (size_t)p->n * sizeof(FPT), cudaMemcpyDeviceToHost, s));
   ISPMV_TRY(cudaStreamSynchronize(s));
-  return ISPMV_OK;
+  return ispmv_plan_status(p);
 }
 
 ISPMV_API int ispmv_plan_spmm(ispmv_plan p, UIN k, const FPT *X, FPT *Y, void *stream) {

@@ -114,57 +114,19 @@ __global__ void k1_order(UIN n, const UIN *__restrict__ permi, const FPT *__rest
   }
 }
 
-// ------------------------------------------------------- AXT NOC, th=1 --
-// Unit = tile of 8 slots of one row (row id: sec).  Each step 8 lanes load
-// one tile (32 lanes = 4 tiles: coalesced 256-byte value loads), reduce it
-// with 3 shuffles, and lane u of the batch collects tile u's sum.
-template <typename VT>
-__global__ void __launch_bounds__(TPB) noc_h1(size_t nunits, UIN useg, const UIN *__restrict__ urow,
-                                              const UIN *__restrict__ col, const VT *__restrict__ val,
-                                              const FPT *__restrict__ x, seg::Out o) {
-  const unsigned lane = threadIdx.x & 31u;
-  const size_t segid = ((size_t)blockIdx.x * TPB + threadIdx.x) >> 5;
-  const size_t u0 = segid * useg;
-  if (u0 >= nunits) return;
-  const size_t u1 = min(u0 + useg, nunits);
-  seg::State st{NO_ROW, 0.0, false};
-  for (size_t ub = u0; ub < u1; ub += 32) {
-    double mine = 0.0;
-#pragma unroll 4
-    for (int j = 0; j < 8; j++) {
-      const size_t t = ub + (size_t)j * 4 + (lane >> 3);
-      double p = 0.0;
-      if (t < u1) {
-        const size_t q = t * 8 + (lane & 7u);
-        p = prod<VT>(ld_stream(val + q), ldg(x + ld_stream(col + q)));
-      }
-      p += __shfl_xor_sync(FULL, p, 4);
-      p += __shfl_xor_sync(FULL, p, 2);
-      p += __shfl_xor_sync(FULL, p, 1);
-      const double tsum = __shfl_sync(FULL, p, (lane & 3u) * 8);
-      if ((lane >> 2) == (unsigned)j) mine = tsum;
-    }
-    const size_t u = ub + lane;
-    const bool live = u < u1;
-    const UIN r = live ? urow[u] : NO_ROW;
-    seg::batch(mine, r, live, st, o, segid);
-  }
-  seg::finish(st, o, segid);
-}
-
 // ------------------------------------------------------- AXT NOC, th>1 --
 // Unit = tile column of th slots (row id: sec[8*T + c]).  th % 4 == 0: each
 // step the warp loads 4 consecutive sub-rows of a tile (32 consecutive
 // slots), adds them per column, and after th/4 steps reduces the 4 partials
 // of each column with 2 shuffles; 4 tiles make a batch of 32 columns.
 template <typename VT>
-__global__ void __launch_bounds__(TPB) noc_hn(size_t nunits, UIN th, UIN useg, const UIN *__restrict__ urow,
+__global__ void __launch_bounds__(TPB) noc_hn(size_t nunits, size_t nseg, UIN th, UIN useg, const UIN *__restrict__ urow,
                                               const UIN *__restrict__ col, const VT *__restrict__ val,
                                               const FPT *__restrict__ x, seg::Out o) {
   const unsigned lane = threadIdx.x & 31u;
   const size_t segid = ((size_t)blockIdx.x * TPB + threadIdx.x) >> 5;
+  if (segid >= nseg) return;
   const size_t u0 = segid * useg;  // useg is a multiple of 32 (4 tiles)
-  if (u0 >= nunits) return;
   const size_t u1 = min(u0 + useg, nunits);
   seg::State st{NO_ROW, 0.0, false};
   const size_t tslots = (size_t)th * 8;
@@ -196,36 +158,6 @@ __global__ void __launch_bounds__(TPB) noc_hn(size_t nunits, UIN th, UIN useg, c
     const bool live = u < u1;
     const UIN r = live ? urow[u] : NO_ROW;
     seg::batch(mine, r, live, st, o, segid);
-  }
-  seg::finish(st, o, segid);
-}
-
-// ----------------------------------------------------------- AXT COM --
-// Unit = slot (packed, CSR order).  Row starts are a bitmap (bit s of
-// heads = a non-empty row starts at slot s); the compressed row of slot s
-// is (#starts <= s) - 1, counted from the segment's base `segh`.
-template <typename VT>
-__global__ void __launch_bounds__(TPB) com_slots(size_t nslots, UIN useg, const UIN *__restrict__ heads,
-                                                 const UIN *__restrict__ segh, const UIN *__restrict__ col,
-                                                 const VT *__restrict__ val, const FPT *__restrict__ x,
-                                                 seg::Out o) {
-  const unsigned lane = threadIdx.x & 31u;
-  const size_t segid = ((size_t)blockIdx.x * TPB + threadIdx.x) >> 5;
-  const size_t s0 = segid * useg;  // multiple of 32
-  if (s0 >= nslots) return;
-  const size_t s1 = min(s0 + useg, nslots);
-  seg::State st{NO_ROW, 0.0, false};
-  UIN cnt = segh[segid];
-  const unsigned le = (lane == 31) ? FULL : ((2u << lane) - 1u);
-  for (size_t sb = s0; sb < s1; sb += 32) {
-    const size_t s = sb + lane;
-    const bool live = s < s1;
-    double p = 0.0;
-    if (live) p = prod<VT>(ld_stream(val + s), ldg(x + ld_stream(col + s)));
-    const UIN w = heads[sb >> 5];
-    const UIN r = live ? cnt + __popc(w & le) - 1u : NO_ROW;
-    cnt += __popc(w);
-    seg::batch(p, r, live, st, o, segid);
   }
   seg::finish(st, o, segid);
 }

@@ -42,6 +42,8 @@ __device__ __forceinline__ void write_row(const Out &o, UIN r, double v) {
 // row (NO_ROW when !live).  Live lanes form a prefix of the warp.
 __device__ __forceinline__ void batch(double p, UIN r, bool live, State &st, const Out &o, size_t segid) {
   const unsigned lane = threadIdx.x & 31u;
+  // a batch past the segment's last unit changes nothing (the open run stays open)
+  if (!__any_sync(FULL, live)) return;
   const UIN rprev = __shfl_up_sync(FULL, r, 1);
   const bool head = (lane == 0) ? (r != st.crow) : (r != rprev);
   // Did the carried run end at the previous batch's last lane?

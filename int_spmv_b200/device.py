@@ -88,14 +88,15 @@ def int_axt_com_h1(bn, bs, log, thw, tn, lenAX, lenRWP, ax, rwp, y, stream=None)
 
 VAL_KINDS = {"f64": abi.VAL_F64, "f32": abi.VAL_F32, "f32lo": abi.VAL_F32_LO16}
 COL_KINDS = {"u32": abi.COL_U32, "d16": abi.COL_D16}
-KERNELS = {"auto": abi.KERNEL_AUTO, "ldg": abi.KERNEL_LDG, "tma": abi.KERNEL_TMA}
+KERNELS = {"auto": abi.KERNEL_AUTO, "ldg": abi.KERNEL_LDG, "tma": abi.KERNEL_TMA, "rows": abi.KERNEL_ROWS}
 
 
-def plan_opts(val="f64", col="u32", kernel="auto", units_per_warp=0, ctas_per_sm=0, lo_tol=0.0) -> abi.PlanOpts:
+def plan_opts(val="f64", col="u32", kernel="auto", units_per_warp=0, ctas_per_sm=0, lo_tol=0.0,
+              variant=0) -> abi.PlanOpts:
     o = abi.PlanOpts()
     load().ispmv_plan_opts_default(C.byref(o))
     o.val_kind, o.col_kind, o.kernel = VAL_KINDS[val], COL_KINDS[col], KERNELS[kernel]
-    o.units_per_warp, o.ctas_per_sm, o.lo_tol = units_per_warp, ctas_per_sm, lo_tol
+    o.units_per_warp, o.ctas_per_sm, o.lo_tol, o.variant = units_per_warp, ctas_per_sm, lo_tol, variant
     return o
 
 
@@ -105,9 +106,10 @@ class Plan:
     False = int_k1 then orderArrayK1)."""
 
     def __init__(self, csr: CSR, fmt: AXC | K1 | AXT | None = None, *, reorder: bool = True, val="f64", col="u32",
-                 kernel="auto", units_per_warp=0, ctas_per_sm=0, lo_tol=0.0, axi: np.ndarray | None = None):
+                 kernel="auto", units_per_warp=0, ctas_per_sm=0, lo_tol=0.0, variant=0,
+                 axi: np.ndarray | None = None):
         lib = load()
-        o = plan_opts(val, col, kernel, units_per_warp, ctas_per_sm, lo_tol)
+        o = plan_opts(val, col, kernel, units_per_warp, ctas_per_sm, lo_tol, variant)
         h = C.c_void_p()
         if fmt is None:
             check(lib.ispmv_plan_csr(C.byref(csr.c), C.byref(o), C.byref(h)), "ispmv_plan_csr")
@@ -144,6 +146,10 @@ class Plan:
         return dict(nrows=i.nrows, nnz=i.nnz, slots=i.slots, device_bytes=i.device_bytes, alg_bytes=i.alg_bytes,
                     format=i.format, val_kind=i.val_kind, col_kind=i.col_kind, kernel=i.kernel, tile_h=i.tile_h,
                     bs=i.bs, name=i.name.decode())
+
+    def status(self) -> int:
+        """ISPMV_ERR_TIMEOUT if a bounded device wait gave up, else 0 (syncs)."""
+        return int(load().ispmv_plan_status(self._h))
 
     def spmv(self, x: torch.Tensor, y: torch.Tensor | None = None, beta: int = 0, stream=None) -> torch.Tensor:
         if x.dtype != torch.float64 or x.numel() != self.n:

@@ -12,7 +12,14 @@ from paritylib import TOL_F32, TOL_F64, assert_parity
 
 pytestmark = pytest.mark.gpu
 
-FORMATS = ["CSR", "AXC", "K1", "K1P", "NOC1", "NOC4", "NOC8", "NOC16", "NOC3", "COM128", "COM256", "COM512"]
+# (format, kernel) pairs a plan supports: "rows" = the row-parallel kernels,
+# "ldg" / "tma" = the slot-stream (or tile-column) kernels with plain loads /
+# 1D bulk copies.
+COMBOS = [("CSR", "rows"), ("CSR", "ldg"), ("CSR", "tma"), ("AXC", "rows"), ("AXC", "ldg"), ("AXC", "tma"),
+          ("K1", "auto"), ("K1P", "auto"), ("NOC1", "ldg"), ("NOC1", "tma"), ("NOC4", "ldg"), ("NOC4", "tma"),
+          ("NOC8", "ldg"), ("NOC8", "tma"), ("NOC16", "ldg"), ("NOC16", "tma"), ("NOC3", "ldg"),
+          ("COM128", "ldg"), ("COM128", "tma"), ("COM256", "ldg"), ("COM512", "tma")]
+KIDS = {"ldg": 1, "tma": 2, "rows": 3}
 
 
 @pytest.fixture(scope="module")
@@ -55,31 +62,46 @@ def check_plan(env, row, col, val, x, fmt, val_kind="f64", beta=0, **kw):
 
 
 @pytest.mark.parametrize("name", golden_names())
-@pytest.mark.parametrize("fmt", FORMATS)
+@pytest.mark.parametrize("fmt,kernel", COMBOS)
 @pytest.mark.parametrize("val_kind", ["f64", "f32"])
-def test_golden(env, name, fmt, val_kind):
+def test_golden(env, name, fmt, kernel, val_kind):
     g = load_golden(name)
     for beta in (0, 1):
-        check_plan(env, g["row"], g["col"], g["val"], g["x"], fmt, val_kind, beta)
+        p, _ = check_plan(env, g["row"], g["col"], g["val"], g["x"], fmt, val_kind, beta, kernel=kernel)
+        if kernel in KIDS:
+            assert p.info["kernel"] == KIDS[kernel]
+    assert p.status() == 0
 
 
-@pytest.mark.parametrize("fmt", FORMATS)
-def test_segment_boundaries(env, fmt):
+@pytest.mark.parametrize("fmt,kernel", COMBOS)
+def test_segment_boundaries(env, fmt, kernel):
     """Small warp segments and long rows: rows span many segments."""
     from int_spmv_b200 import matrices as M
     row, col, val = M.random_csr(3001, 9, rl_max=700, empty_frac=0.2)
     x = M.uniform_x(3001, 9)
     for upw in (32, 64, 0):
-        check_plan(env, row, col, val, x, fmt, units_per_warp=upw)
+        check_plan(env, row, col, val, x, fmt, units_per_warp=upw, kernel=kernel)
 
 
-@pytest.mark.parametrize("fmt", ["NOC1", "NOC4", "COM128", "CSR", "K1P"])
-def test_deterministic_and_host_e2e(env, fmt):
+@pytest.mark.parametrize("fmt", ["COM128", "NOC1", "AXC", "CSR"])
+@pytest.mark.parametrize("variant", list(range(8)))
+def test_stream_variants(env, fmt, variant):
+    from int_spmv_b200 import matrices as M
+    row, col, val = M.random_csr(7001, 12, rl_max=90, empty_frac=0.1)
+    x = M.uniform_x(7001, 12)
+    for ctas in (1, 2, 3):
+        check_plan(env, row, col, val, x, fmt, kernel="ldg", variant=variant)
+        check_plan(env, row, col, val, x, fmt, kernel="tma", ctas_per_sm=ctas)
+
+
+@pytest.mark.parametrize("fmt,kernel", [("NOC1", "ldg"), ("NOC4", "tma"), ("COM128", "ldg"), ("COM128", "tma"),
+                                        ("CSR", "rows"), ("K1P", "auto")])
+def test_deterministic_and_host_e2e(env, fmt, kernel):
     torch, D, F, orc = env
     from int_spmv_b200 import matrices as M
     row, col, val = M.random_csr(20000, 4, rl_max=60, empty_frac=0.05)
     x = M.uniform_x(20000, 4)
-    p, xt = check_plan(env, row, col, val, x, fmt)
+    p, xt = check_plan(env, row, col, val, x, fmt, kernel=kernel)
     a = p.spmv(xt).cpu().numpy()
     b = p.spmv(xt).cpu().numpy()
     assert np.array_equal(a, b)  # no atomics on the plan path: bitwise repeatable
@@ -96,11 +118,11 @@ def poisson512(env):
     return row, col, val, M.uniform_x(len(row) - 1, 0)
 
 
-@pytest.mark.parametrize("fmt", ["CSR", "NOC1"])
-def test_poisson512(env, poisson512, fmt):
+@pytest.mark.parametrize("fmt,kernel", [("CSR", "rows"), ("NOC1", "ldg"), ("NOC1", "tma"), ("COM128", "ldg")])
+def test_poisson512(env, poisson512, fmt, kernel):
     row, col, val, x = poisson512
     assert len(row) - 1 == 262144 and len(col) == 1308672
-    check_plan(env, row, col, val, x, fmt)
+    check_plan(env, row, col, val, x, fmt, kernel=kernel)
 
 
 @pytest.fixture(scope="module")
@@ -110,9 +132,13 @@ def powerlaw4m(env):
     return row, col, val, M.uniform_x(4_000_000, 1)
 
 
-@pytest.mark.parametrize("fmt", ["CSR", "AXC", "K1P", "NOC1", "NOC4", "NOC8", "COM128", "COM512"])
-def test_powerlaw_4m(env, powerlaw4m, fmt):
+@pytest.mark.parametrize("fmt,kernel", [("CSR", "rows"), ("CSR", "ldg"), ("AXC", "rows"), ("AXC", "ldg"),
+                                        ("K1P", "auto"), ("NOC1", "ldg"), ("NOC1", "tma"), ("NOC4", "ldg"),
+                                        ("NOC4", "tma"), ("NOC8", "tma"), ("COM128", "ldg"), ("COM128", "tma"),
+                                        ("COM512", "ldg")])
+def test_powerlaw_4m(env, powerlaw4m, fmt, kernel):
     row, col, val, x = powerlaw4m
-    check_plan(env, row, col, val, x, fmt)
-    if fmt in ("COM128", "NOC1"):
-        check_plan(env, row, col, val, x, fmt, val_kind="f32")
+    p, _ = check_plan(env, row, col, val, x, fmt, kernel=kernel)
+    assert p.status() == 0
+    if (fmt, kernel) in (("COM128", "ldg"), ("NOC1", "ldg")):
+        check_plan(env, row, col, val, x, fmt, val_kind="f32", kernel=kernel)
