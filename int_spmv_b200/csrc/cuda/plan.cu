@@ -17,6 +17,7 @@
 //           (pk::axc_rows): the row-parallel kernels.
 //   K1      val/col column-major per chunk, chp, nmc, permi (pk::k1_chunks).
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -48,6 +49,10 @@ struct ispmv_plan_s {
   UIN *rec_row = nullptr;
   double *rec_sum = nullptr;
   int *status = nullptr;
+  sss::Narrow narrow{};   // D16 / LO side streams (stream path only)
+  sss::XWin xw{};         // x bands staged in shared memory (variants >= 8)
+  double lo_frac = 0.0;   // fraction of slots carrying a lo-word
+  size_t esc_batches = 0; // D16 batches kept as u32 columns
   FPT *hx = nullptr, *hy = nullptr;  // device staging of ispmv_plan_spmv_host
   std::vector<void *> owned;
   ispmv_plan_info info{};
@@ -80,6 +85,19 @@ int dev_alloc(ispmv_plan_s *p, size_t n, T **d) {
 
 size_t vbytes(const ispmv_plan_s *p) { return p->opts.val_kind == ISPMV_VAL_F64 ? 8 : 4; }
 
+// The reduced-byte side streams exist only on the slot-stream path.
+bool narrow_kinds(const ispmv_plan_s *p) {
+  return p->opts.val_kind == ISPMV_VAL_F32_LO16 || p->opts.col_kind == ISPMV_COL_D16;
+}
+
+uint16_t to_bf16(float f) {  // round to nearest even
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u) return (uint16_t)(u >> 16);
+  u += 0x7fffu + ((u >> 16) & 1u);
+  return (uint16_t)(u >> 16);
+}
+
 int upload_values(ispmv_plan_s *p, const std::vector<double> &v) {
   if (p->opts.val_kind == ISPMV_VAL_F64) {
     double *d;
@@ -87,6 +105,7 @@ int upload_values(ispmv_plan_s *p, const std::vector<double> &v) {
     p->val = d;
     return ISPMV_OK;
   }
+  // FP32 (and the hi part of FP32 + lo-word)
   std::vector<float> f(v.size());
   for (size_t i = 0; i < v.size(); i++) f[i] = (float)v[i];
   float *d;
@@ -106,7 +125,13 @@ void finish_info(ispmv_plan_s *p, const char *name) {
   i.kernel = p->opts.kernel;
   i.tile_h = p->th;
   i.bs = p->bs;
-  const double bv = (double)vbytes(p), bi = 4.0;
+  // b_val: 8 | 4 | 4 + 2*(lo-word fraction); b_idx: 4 | 2 + 4*(batch bases + escaped columns)/nnz
+  double bv = (double)vbytes(p), bi = 4.0;
+  if (p->opts.val_kind == ISPMV_VAL_F32_LO16) bv = 4.0 + 2.0 * p->lo_frac;
+  if (p->opts.col_kind == ISPMV_COL_D16 && p->slots_pad) {
+    const double batches = (double)(p->slots_pad / 128);
+    bi = 2.0 + (4.0 * batches + 128.0 * 4.0 * (double)p->esc_batches) / std::max(1.0, (double)p->nnz);
+  }
   i.alg_bytes = (double)p->nnz * (bv + bi) + (double)p->n * 16.0 + 4.0 * ((double)p->n + 1.0);
   snprintf(i.name, sizeof i.name, "%s", name);
 }
@@ -125,8 +150,8 @@ int begin(const ispmv_plan_opts *o, ispmv_plan_s **out) {
   if (!p) return ISPMV_ERR_OOM;
   if (o) p->opts = *o;
   else ispmv_plan_opts_default(&p->opts);
-  if ((p->opts.val_kind != ISPMV_VAL_F64 && p->opts.val_kind != ISPMV_VAL_F32) || p->opts.col_kind != ISPMV_COL_U32 ||
-      p->opts.kernel < 0 || p->opts.kernel > ISPMV_KERNEL_ROWS) {
+  if (p->opts.val_kind < ISPMV_VAL_F64 || p->opts.val_kind > ISPMV_VAL_F32_LO16 || p->opts.col_kind < ISPMV_COL_U32 ||
+      p->opts.col_kind > ISPMV_COL_D16 || p->opts.kernel < 0 || p->opts.kernel > ISPMV_KERNEL_ROWS) {
     delete p;
     return ISPMV_ERR_UNSUPPORTED;
   }
@@ -165,6 +190,59 @@ size_t seg_slots_of(const ispmv_plan_s *p, size_t upu) {
   return std::max(SS, ((size_t)p->opts.units_per_warp * upu + SS - 1) / SS * SS);
 }
 
+// x-window kernel variants: (warps per CTA, shared doubles per CTA, segment slots)
+struct XwCfg { int warps; UIN cap; size_t seg; };
+bool xw_variant(int v, XwCfg *c) {
+  switch (v) {
+    case 8: *c = {16, 4096, 1024}; return true;
+    case 9: *c = {16, 8192, 1024}; return true;
+    case 10: *c = {8, 2048, 1024}; return true;
+    case 11: *c = {16, 6144, 2048}; return true;
+    default: return false;
+  }
+}
+
+// Picks up to 3 diagonal bands (offset, half-width) of col - row from a
+// deterministic sample of the nonzeros: the densest interval that fits the
+// budget, then the densest of what is left, while a band holds >= 5% of the
+// sample.  `span` is the typical row range of one CTA.
+void choose_windows(const str_matCSR *csr, UIN cap, double span, sss::XWin *xw) {
+  xw->nwin = 0;
+  const size_t nnz = csr->nnz, S = std::min<size_t>(nnz, 1u << 21);
+  if (!S) return;
+  std::vector<long long> d(S);
+  const double stride = (double)nnz / (double)S;
+  for (size_t i = 0, r = 0; i < S; i++) {
+    const size_t j = (size_t)(i * stride);
+    while (csr->row[r + 1] <= j) r++;
+    d[i] = (long long)csr->col[j] - (long long)r;
+  }
+  std::sort(d.begin(), d.end());
+  std::vector<char> used(S, 0);
+  long long budget = (long long)cap;
+  for (int k = 0; k < sss::XW_MAX; k++) {
+    const long long hmax = (budget - (long long)span) / 2;
+    if (hmax < 1) break;
+    const long long W = 2 * hmax + 1;
+    size_t best = 0, ba = 0, bb = 0, cnt = 0;
+    for (size_t a = 0, b = 0; a < S; a++) {  // [a, b): points with d in [d[a], d[a] + W)
+      if (b < a) { b = a; cnt = 0; }
+      while (b < S && d[b] < d[a] + W) { cnt += !used[b]; b++; }
+      if (cnt > best) { best = cnt; ba = a; bb = b; }
+      cnt -= !used[a];
+    }
+    if (best * 20 < S) break;
+    long long lo = d[ba], hi = d[ba];
+    for (size_t i = ba; i < bb; i++)
+      if (!used[i]) { lo = std::min(lo, d[i]); hi = std::max(hi, d[i]); used[i] = 1; }
+    const long long center = (lo + hi) / 2, half = (hi - lo + 1) / 2 + 1;
+    xw->off[xw->nwin] = center;
+    xw->half[xw->nwin] = half;
+    xw->nwin++;
+    budget -= (long long)span + 2 * half;
+  }
+}
+
 // The stream path: `v`/`c` the slot streams (length p->slots), `start[r]`
 // the first slot of row r (rows with no slot are skipped).
 int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v, std::vector<UIN> &c,
@@ -174,7 +252,7 @@ int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v,
   v.resize(p->slots_pad, 0.0);
   c.resize(p->slots_pad, 0);
   TRY(upload_values(p, v));
-  TRY(dev_upload(p, c.data(), c.size(), &p->col));
+  if (p->opts.col_kind == ISPMV_COL_U32) TRY(dev_upload(p, c.data(), c.size(), &p->col));
   std::vector<UIN> heads(p->slots_pad / 32, 0), rowmap;
   bool any_empty = false;
   for (UIN r = 0; r < p->n; r++) {
@@ -186,7 +264,9 @@ int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v,
     heads[q >> 5] |= 1u << (q & 31);
     rowmap.push_back(r);
   }
-  p->seg_slots = seg_slots_of(p, 1);
+  XwCfg xc;
+  const bool xwv = p->opts.kernel == ISPMV_KERNEL_LDG && !narrow_kinds(p) && xw_variant(p->opts.variant, &xc);
+  p->seg_slots = xwv && p->opts.units_per_warp <= 0 ? xc.seg : seg_slots_of(p, 1);
   p->nseg = (p->slots_pad + p->seg_slots - 1) / p->seg_slots;
   std::vector<UIN> segh(std::max<size_t>(1, p->nseg), 0);
   UIN acc = 0;
@@ -195,12 +275,77 @@ int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v,
     for (; w < wend; w++) acc += __builtin_popcount(heads[w]);
     segh[sg] = acc;
   }
+  if (p->opts.col_kind == ISPMV_COL_D16) {
+    // per 128-slot batch: base = the smallest column among nonzero values;
+    // deltas to it in 16 bits, or the batch's u32 columns when the span is wider
+    const size_t nb = p->slots_pad / 128;
+    std::vector<UIN> cmeta(nb), esc;
+    std::vector<uint16_t> c16(p->slots_pad, 0);
+    for (size_t b = 0; b < nb; b++) {
+      UIN lo = 0xFFFFFFFFu, hi = 0;
+      for (size_t q = b * 128; q < b * 128 + 128; q++)
+        if (v[q] != 0.0) { lo = std::min(lo, c[q]); hi = std::max(hi, c[q]); }
+      if (lo == 0xFFFFFFFFu) lo = hi = 0;
+      if (hi - lo <= 0xFFFFu && lo < sss::ESCAPE) {
+        cmeta[b] = lo;
+        for (size_t q = b * 128; q < b * 128 + 128; q++) c16[q] = v[q] != 0.0 ? (uint16_t)(c[q] - lo) : 0;
+      } else {
+        cmeta[b] = sss::ESCAPE | (UIN)p->esc_batches++;
+        esc.insert(esc.end(), c.begin() + b * 128, c.begin() + b * 128 + 128);
+      }
+    }
+    uint16_t *d16; UIN *dm, *de;
+    TRY(dev_upload(p, c16.data(), c16.size(), &d16));
+    TRY(dev_upload(p, cmeta.data(), cmeta.size(), &dm));
+    TRY(dev_upload(p, esc.data(), esc.size(), &de));
+    p->narrow.col16 = d16; p->narrow.cmeta = dm; p->narrow.esc = de;
+  }
+  if (p->opts.val_kind == ISPMV_VAL_F32_LO16) {
+    // rows whose FP32 rounding error, relative to their row sum, exceeds
+    // lo_tol get a BF16 residual; it is stored for every segment they touch
+    const double tol = p->opts.lo_tol > 0 ? p->opts.lo_tol : 1e-6;
+    std::vector<char> segflag(p->nseg, 0);
+    for (UIN r = 0; r < p->n; r++) {
+      double err = 0.0, sum = 0.0;
+      for (UIN j = csr->row[r]; j < csr->row[r + 1]; j++) {
+        err += std::fabs(csr->val[j] - (double)(float)csr->val[j]);
+        sum += csr->val[j];
+      }
+      if (csr->row[r + 1] == csr->row[r] || err <= tol * std::fabs(sum)) continue;
+      const size_t a = start[r], e = start[r] + (csr->row[r + 1] - csr->row[r]);
+      for (size_t sg = a / p->seg_slots; sg <= (e - 1) / p->seg_slots && sg < p->nseg; sg++) segflag[sg] = 1;
+    }
+    std::vector<UIN> off(p->nseg, NO_ROW);
+    std::vector<uint16_t> lo;
+    for (size_t sg = 0; sg < p->nseg; sg++) {
+      if (!segflag[sg]) continue;
+      off[sg] = (UIN)lo.size();
+      const size_t a = sg * p->seg_slots, e = std::min(p->slots_pad, a + p->seg_slots);
+      for (size_t q = a; q < e; q++) lo.push_back(to_bf16((float)(v[q] - (double)(float)v[q])));
+    }
+    p->lo_frac = p->slots ? (double)lo.size() / (double)p->slots_pad : 0.0;
+    uint16_t *dl; UIN *dof;
+    TRY(dev_upload(p, lo.data(), lo.size(), &dl));
+    TRY(dev_upload(p, off.data(), off.size(), &dof));
+    p->narrow.lo16 = dl; p->narrow.lo_off = dof;
+  }
   TRY(dev_upload(p, heads.data(), heads.size(), &p->heads));
   TRY(dev_upload(p, segh.data(), segh.size(), &p->segh));
   if (any_empty) TRY(dev_upload(p, rowmap.data(), rowmap.size(), &p->rowmap));
+  if (xwv) {
+    const double rows_per_slot = (double)rowmap.size() / (double)std::max<size_t>(1, p->slots);
+    choose_windows(csr, xc.cap, rows_per_slot * (double)(xc.warps * p->seg_slots), &p->xw);
+    p->xw.cap = xc.cap;
+    p->xw.rowmap = p->rowmap;
+    p->xw.n = p->n;
+    p->xw.nrows_c = (UIN)rowmap.size();
+  }
   TRY(empty_rows(p, csr));
   TRY(alloc_records(p));
-  p->info.device_bytes = (uint64_t)p->slots_pad * (vbytes(p) + 4) + p->slots_pad / 8;
+  p->info.device_bytes = (uint64_t)p->slots_pad * vbytes(p) + p->slots_pad / 8 +
+                         (p->opts.col_kind == ISPMV_COL_D16 ? p->slots_pad * 2 + p->slots_pad / 32 + p->esc_batches * 512
+                                                           : p->slots_pad * 4) +
+                         (uint64_t)(p->lo_frac * (double)p->slots_pad * 2.0);
   return ISPMV_OK;
 }
 
@@ -231,8 +376,10 @@ ISPMV_API int ispmv_plan_csr(const str_matCSR *csr, const ispmv_plan_opts *o, is
   p->nnz = csr->nnz;
   p->slots = csr->nnz;
   int st = ISPMV_OK;
+  if (narrow_kinds(p) && p->opts.kernel == ISPMV_KERNEL_AUTO) p->opts.kernel = ISPMV_KERNEL_LDG;
   if (p->opts.kernel == ISPMV_KERNEL_AUTO || p->opts.kernel == ISPMV_KERNEL_ROWS) {
     // the naive CSR product on the GPU: L lanes per row
+    if (narrow_kinds(p)) { ispmv_plan_destroy(p); return ISPMV_ERR_UNSUPPORTED; }
     p->opts.kernel = ISPMV_KERNEL_ROWS;
     p->path = P_ROWS;
     const double mean = (double)csr->nnz / csr->nrows;
@@ -267,8 +414,10 @@ ISPMV_API int ispmv_plan_axc(const str_matCSR *csr, const str_matAXC *axc, const
   std::vector<UIN> c(axi, axi + p->slots);
   for (size_t s = 0; s < p->slots; s++) v[s] = axc->ax[(s / 8) * 16 + s % 8];
   int st = ISPMV_OK;
+  if (narrow_kinds(p) && p->opts.kernel == ISPMV_KERNEL_AUTO) p->opts.kernel = ISPMV_KERNEL_LDG;
   if (p->opts.kernel == ISPMV_KERNEL_AUTO || p->opts.kernel == ISPMV_KERNEL_ROWS) {
     // the reference's row loop (M:711-732): 8 lanes per row over its bricks
+    if (narrow_kinds(p)) { ispmv_plan_destroy(p); return ISPMV_ERR_UNSUPPORTED; }
     p->opts.kernel = ISPMV_KERNEL_ROWS;
     p->path = P_ROWS;
     std::vector<UIN> bptr((size_t)p->n + 1);
@@ -294,6 +443,10 @@ ISPMV_API int ispmv_plan_k1(const str_matCSR *csr, const str_matK1 *k1, int reor
     return ISPMV_ERR_ARG;
   ispmv_plan_s *p;
   TRY(begin(o, &p));
+  if (narrow_kinds(p)) {
+    delete p;
+    return ISPMV_ERR_UNSUPPORTED;
+  }
   p->fmt = reorder ? F_K1P : F_K1;
   p->path = P_K1;
   p->opts.kernel = ISPMV_KERNEL_ROWS;
@@ -356,6 +509,7 @@ ISPMV_API int ispmv_plan_axt(const str_matCSR *csr, const str_matAXT *axt, const
   } else {
     // tile columns: the unit engine on the reference's per-column rows
     p->path = P_UNITS;
+    if (narrow_kinds(p)) st = ISPMV_ERR_UNSUPPORTED;
     size_t used = 0;
     for (UIN r = 0; r < p->n; r++) used += ((size_t)csr->rl[r] + th - 1) / th * th;
     p->slots = (size_t)axt->lenAX / 2;
@@ -421,6 +575,32 @@ int run_stream(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
   const VT *val = static_cast<const VT *>(p->val);
   size_t nslots = p->slots, spad = p->slots_pad, sslots = p->seg_slots, nseg = p->nseg;
   const UIN *col = p->col, *heads = p->heads, *segh = p->segh;
+  if (narrow_kinds(p)) {
+    const unsigned g = (unsigned)((nseg * 32 + 255) / 256);
+    const bool lo = p->opts.val_kind == ISPMV_VAL_F32_LO16, d16 = p->opts.col_kind == ISPMV_COL_D16;
+    if (lo && d16)
+      sss::stream_narrow<VT, true, true><<<g, 256, 0, s>>>(nslots, spad, sslots, nseg, val, col, heads, segh, p->narrow, x, o);
+    else if (lo)
+      sss::stream_narrow<VT, true, false><<<g, 256, 0, s>>>(nslots, spad, sslots, nseg, val, col, heads, segh, p->narrow, x, o);
+    else
+      sss::stream_narrow<VT, false, true><<<g, 256, 0, s>>>(nslots, spad, sslots, nseg, val, col, heads, segh, p->narrow, x, o);
+    return check_launch("stream_narrow");
+  }
+  XwCfg xc;
+  if (p->opts.kernel == ISPMV_KERNEL_LDG && xw_variant(p->opts.variant, &xc)) {
+    const size_t smem = (size_t)xc.cap * sizeof(double);
+    const unsigned g = (unsigned)((nseg + xc.warps - 1) / xc.warps);
+    if (xc.warps == 16) {
+      ISPMV_TRY(cudaFuncSetAttribute((const void *)sss::stream_xw<VT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+      sss::stream_xw<VT, 16><<<g, 512, smem, s>>>(nslots, spad, sslots, nseg, val, col, heads, segh, p->xw, x, o);
+    } else {
+      ISPMV_TRY(cudaFuncSetAttribute((const void *)sss::stream_xw<VT, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+      sss::stream_xw<VT, 8><<<g, 256, smem, s>>>(nslots, spad, sslots, nseg, val, col, heads, segh, p->xw, x, o);
+    }
+    return check_launch("stream_xw");
+  }
   if (p->opts.kernel == ISPMV_KERNEL_TMA) {
     int *status = p->status;
     void *args[] = {&nslots, &spad, &sslots, &nseg, &val, &col, &heads, &segh, (void *)&x, &o, &status};

@@ -258,6 +258,192 @@ __global__ void __launch_bounds__(256, MINB) stream_ldg(size_t nslots, size_t ns
   finish(st, o);
 }
 
+// x windows: up to XW_MAX diagonal bands of x staged in shared memory.
+// A CTA's warps own consecutive segments, so its rows form one range
+// [r0, r1]; band k covers columns [r0 + off_k - h_k, r1 + off_k + h_k]
+// (clipped to [0, n) and to the CTA's share of shared memory).  The plan
+// picks the bands from the histogram of col - row.  A gather whose column
+// falls in a band reads shared memory; any other column reads x through
+// L1/L2, so the result does not depend on the bands.
+constexpr int XW_MAX = 3;
+struct XWin {
+  int nwin;
+  long long off[XW_MAX];
+  long long half[XW_MAX];
+  UIN cap;             // doubles of shared memory per CTA
+  const UIN *rowmap;   // compressed -> real rows (nullptr: identity)
+  UIN n;               // rows (= columns)
+  UIN nrows_c;         // compressed rows (non-empty)
+};
+
+struct WinState {
+  long long lo[XW_MAX];
+  UIN len[XW_MAX];
+  UIN base[XW_MAX];  // offset of band k in shared memory
+};
+
+__device__ __forceinline__ double xw_load(const WinState &w, int nwin, const double *sx, const FPT *__restrict__ x,
+                                          UIN c) {
+#pragma unroll
+  for (int k = 0; k < XW_MAX; k++) {
+    if (k < nwin) {
+      const long long d = (long long)c - w.lo[k];
+      if (d >= 0 && d < (long long)w.len[k]) return sx[w.base[k] + (UIN)d];
+    }
+  }
+  return __ldg(x + c);
+}
+
+template <typename VT, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, 48 / WARPS) stream_xw(size_t nslots, size_t nslots_pad, size_t seg_slots,
+                                                           size_t nseg, const VT *__restrict__ val,
+                                                           const UIN *__restrict__ col, const UIN *__restrict__ heads,
+                                                           const UIN *__restrict__ segh, XWin xw,
+                                                           const FPT *__restrict__ x, seg::Out o) {
+  constexpr int SPL = 4, BT = 128;
+  extern __shared__ __align__(16) double sx[];
+  __shared__ WinState sw;
+  const unsigned lane = threadIdx.x & 31u;
+  const size_t seg0 = (size_t)blockIdx.x * WARPS;
+  const size_t segid = seg0 + (threadIdx.x >> 5);
+  // the CTA's row range, from the start counts of its first and one-past-last segments
+  if (threadIdx.x == 0) {
+    const size_t segl = min(seg0 + WARPS, nseg);
+    UIN c0 = segh[seg0];
+    c0 = c0 > 0 ? c0 - 1 : 0;                                    // the run open at the first slot
+    UIN c1 = segl < nseg ? segh[segl] : xw.nrows_c;              // rows started before the end
+    c1 = c1 > 0 ? c1 - 1 : 0;
+    if (c1 >= xw.nrows_c) c1 = xw.nrows_c ? xw.nrows_c - 1 : 0;
+    const long long r0 = xw.rowmap ? xw.rowmap[c0] : c0, r1 = xw.rowmap ? xw.rowmap[c1] : c1;
+    UIN used = 0;
+#pragma unroll
+    for (int k = 0; k < XW_MAX; k++) {
+      long long lo = r0 + xw.off[k] - xw.half[k], hi = r1 + xw.off[k] + xw.half[k] + 1;
+      lo = lo < 0 ? 0 : lo;
+      hi = hi > (long long)xw.n ? (long long)xw.n : hi;
+      long long len = (k < xw.nwin && hi > lo) ? hi - lo : 0;
+      if (len > (long long)(xw.cap - used)) len = xw.cap - used;  // shared memory budget
+      sw.lo[k] = lo;
+      sw.len[k] = (UIN)len;
+      sw.base[k] = used;
+      used += (UIN)len;
+    }
+  }
+  __syncthreads();
+  WinState w;
+#pragma unroll
+  for (int k = 0; k < XW_MAX; k++) {
+    w.lo[k] = sw.lo[k];
+    w.len[k] = sw.len[k];
+    w.base[k] = sw.base[k];
+    for (UIN i = threadIdx.x; i < w.len[k]; i += WARPS * 32) sx[w.base[k] + i] = __ldg(x + w.lo[k] + i);
+  }
+  __syncthreads();
+  if (segid >= nseg) return;
+  const size_t s0 = segid * seg_slots;
+  const size_t s1 = min(s0 + seg_slots, nslots_pad);
+  const int nbat = (int)((s1 - s0) / BT);
+  Run st;
+  begin(st, o, segid, segh[segid], __ldg(heads + (s0 >> 5)));
+  for (int j = 0; j < nbat; j++) {
+    const size_t b = s0 + (size_t)j * BT, sl = b + SPL * lane;
+    Vals<VT, SPL> v;
+    v.get(val, sl);
+    Cols<SPL> c;
+    c.get(col, sl);
+    Words<SPL> h;
+    get_words<SPL>(h, heads, b);
+    double p[SPL];
+#pragma unroll
+    for (int k = 0; k < SPL; k++) p[k] = pk::prod<VT>(v[k], xw_load(w, xw.nwin, sx, x, c[k]));
+    if (sl + SPL > nslots) {
+#pragma unroll
+      for (int k = 0; k < SPL; k++)
+        if (sl + k >= nslots) p[k] = 0.0;
+    }
+    batch<SPL>(p, h, st, o);
+  }
+  finish(st, o);
+}
+
+// Reduced-byte streams (4 slots per lane, no prefetch, 6 CTAs/SM):
+//   LO   FP32 values plus, in segments whose rows need it, a BF16 residual
+//        lo-word per slot: value = hi + lo, multiplied by x in FP64.
+//   D16  16-bit column deltas from a per-batch base column (cmeta[b]); a
+//        batch whose span does not fit 16 bits has its u32 columns in `esc`
+//        (cmeta[b] = ESCAPE | escape index).
+struct Narrow {
+  const uint16_t *col16;  // D16 deltas
+  const UIN *cmeta;       // D16 per-batch base or escape index
+  const UIN *esc;         // D16 escaped batches' columns (128 each)
+  const uint16_t *lo16;   // LO residuals of flagged segments, compacted
+  const UIN *lo_off;      // LO per-segment offset into lo16, or NO_ROW
+};
+constexpr UIN ESCAPE = 0x80000000u;
+
+__device__ __forceinline__ double bf16_to_double(uint16_t h) { return (double)__uint_as_float((UIN)h << 16); }
+
+template <typename VT, bool LO, bool D16>
+__global__ void __launch_bounds__(256, 6) stream_narrow(size_t nslots, size_t nslots_pad, size_t seg_slots,
+                                                        size_t nseg, const VT *__restrict__ val,
+                                                        const UIN *__restrict__ col, const UIN *__restrict__ heads,
+                                                        const UIN *__restrict__ segh, Narrow nw,
+                                                        const FPT *__restrict__ x, seg::Out o) {
+  constexpr int SPL = 4, BT = 128;
+  const unsigned lane = threadIdx.x & 31u;
+  const size_t segid = ((size_t)blockIdx.x * 256 + threadIdx.x) >> 5;
+  if (segid >= nseg) return;
+  const size_t s0 = segid * seg_slots;
+  const size_t s1 = min(s0 + seg_slots, nslots_pad);
+  const int nbat = (int)((s1 - s0) / BT);
+  Run st;
+  begin(st, o, segid, segh[segid], __ldg(heads + (s0 >> 5)));
+  UIN lo_base = NO_ROW;
+  if (LO) lo_base = __ldg(nw.lo_off + segid);
+  for (int j = 0; j < nbat; j++) {
+    const size_t b = s0 + (size_t)j * BT, sl = b + SPL * lane;
+    Vals<VT, SPL> v;
+    v.get(val, sl);
+    UIN c[SPL];
+    if (D16) {
+      const UIN m = __ldg(nw.cmeta + (b >> 7));
+      if (m & ESCAPE) {
+        const uint4 e = ld_stream(reinterpret_cast<const uint4 *>(nw.esc + (size_t)(m & ~ESCAPE) * BT + SPL * lane));
+        c[0] = e.x; c[1] = e.y; c[2] = e.z; c[3] = e.w;
+      } else {
+        const uint2 d = ld_stream(reinterpret_cast<const uint2 *>(nw.col16 + sl));
+        c[0] = m + (d.x & 0xFFFFu); c[1] = m + (d.x >> 16); c[2] = m + (d.y & 0xFFFFu); c[3] = m + (d.y >> 16);
+      }
+    } else {
+      const uint4 e = ld_stream(reinterpret_cast<const uint4 *>(col + sl));
+      c[0] = e.x; c[1] = e.y; c[2] = e.z; c[3] = e.w;
+    }
+    Words<SPL> h;
+    get_words<SPL>(h, heads, b);
+    double p[SPL];
+    if (LO && lo_base != NO_ROW) {
+      const uint2 l = ld_stream(reinterpret_cast<const uint2 *>(nw.lo16 + lo_base + (sl - s0)));
+      const uint16_t lw[4] = {(uint16_t)(l.x & 0xFFFFu), (uint16_t)(l.x >> 16), (uint16_t)(l.y & 0xFFFFu),
+                              (uint16_t)(l.y >> 16)};
+#pragma unroll
+      for (int k = 0; k < SPL; k++) {
+        const double xv = ldg(x + c[k]);
+        p[k] = fma(bf16_to_double(lw[k]), xv, (double)v[k] * xv);  // residual corrected in FP64
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < SPL; k++) p[k] = pk::prod<VT>(v[k], ldg(x + c[k]));
+    }
+    if (sl + SPL > nslots) {
+#pragma unroll
+      for (int k = 0; k < SPL; k++)
+        if (sl + k >= nslots) p[k] = 0.0;
+    }
+    batch<SPL>(p, h, st, o);
+  }
+  finish(st, o);
+}
+
 // Staged kernel: persistent warps, each with a ring of STAGES 512-slot
 // stages filled by 1D bulk copies (values, columns, bitmap).
 constexpr int SS = 512;

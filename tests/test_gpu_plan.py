@@ -45,9 +45,9 @@ def make_plan(F, D, csr, x, fmt, **kw):
     raise ValueError(fmt)
 
 
-def check_plan(env, row, col, val, x, fmt, val_kind="f64", beta=0, **kw):
+def check_plan(env, row, colidx, val, x, fmt, val_kind="f64", beta=0, **kw):
     torch, D, F, orc = env
-    csr = F.CSR(row, col, val)
+    csr = F.CSR(row, colidx, val)
     p = make_plan(F, D, csr, x, fmt, val=val_kind, **kw)
     n = csr.n
     xt = torch.from_numpy(np.ascontiguousarray(x)).cuda()
@@ -55,8 +55,8 @@ def check_plan(env, row, col, val, x, fmt, val_kind="f64", beta=0, **kw):
     yt = torch.from_numpy(y0.copy()).cuda()
     p.spmv(xt, yt, beta=beta)
     y = yt.cpu().numpy()
-    ref = orc.cf_csr(row, col, val, x) + (y0 if beta else 0.0)
-    absax = orc.abs_csr(row, col, val, x) + (np.abs(y0) * 1e-4 if beta else 0.0)
+    ref = orc.cf_csr(row, colidx, val, x) + (y0 if beta else 0.0)
+    absax = orc.abs_csr(row, colidx, val, x) + (np.abs(y0) * 1e-4 if beta else 0.0)
     assert_parity(y, ref, absax, TOL_F64 if val_kind == "f64" else TOL_F32, what=f"{fmt}/{val_kind}/beta{beta}")
     return p, xt
 
@@ -84,7 +84,7 @@ def test_segment_boundaries(env, fmt, kernel):
 
 
 @pytest.mark.parametrize("fmt", ["COM128", "NOC1", "AXC", "CSR"])
-@pytest.mark.parametrize("variant", list(range(8)))
+@pytest.mark.parametrize("variant", list(range(12)))
 def test_stream_variants(env, fmt, variant):
     from int_spmv_b200 import matrices as M
     row, col, val = M.random_csr(7001, 12, rl_max=90, empty_frac=0.1)
@@ -142,3 +142,49 @@ def test_powerlaw_4m(env, powerlaw4m, fmt, kernel):
     assert p.status() == 0
     if (fmt, kernel) in (("COM128", "ldg"), ("NOC1", "ldg")):
         check_plan(env, row, col, val, x, fmt, val_kind="f32", kernel=kernel)
+
+
+STREAM_FMTS = [("COM128", "ldg"), ("NOC1", "ldg"), ("AXC", "ldg"), ("CSR", "ldg")]
+NARROW = [("f32lo", "u32"), ("f32", "d16"), ("f64", "d16"), ("f32lo", "d16")]
+
+
+@pytest.mark.parametrize("name", golden_names())
+@pytest.mark.parametrize("fmt,kernel", STREAM_FMTS)
+@pytest.mark.parametrize("val_kind,col_kind", NARROW)
+def test_precision_forms_golden(env, name, fmt, kernel, val_kind, col_kind):
+    g = load_golden(name)
+    for beta in (0, 1):
+        check_plan(env, g["row"], g["col"], g["val"], g["x"], fmt, val_kind, beta, kernel=kernel, col=col_kind)
+
+
+@pytest.mark.parametrize("fmt,kernel", STREAM_FMTS)
+def test_precision_forms_banded_and_random(env, fmt, kernel):
+    """Banded rows (16-bit deltas fit) and random rows (batches escape to u32);
+    with every row carrying a lo-word the FP32 + BF16 form is within 1e-8."""
+    torch, D, F, orc = env
+    from int_spmv_b200 import matrices as M
+    rng = np.random.default_rng(3)
+    mats = [M.fem_banded(5000, rng), M.random_csr(6000, 21, rl_max=50, empty_frac=0.05), M.stencil27(20, seed=2)]
+    for row, col, val in mats:
+        x = M.uniform_x(len(row) - 1, 8)
+        for vk, ck in NARROW:
+            p, _ = check_plan(env, row, col, val, x, fmt, vk, kernel=kernel, col=ck)
+            assert p.info["col_kind"] == (1 if ck == "d16" else 0)
+        # all rows flagged: residual-corrected values
+        csr = F.CSR(row, col, val)
+        p = make_plan(F, D, csr, x, fmt, val="f32lo", kernel=kernel, lo_tol=1e-300)
+        y = p.spmv(torch.from_numpy(x).cuda()).cpu().numpy()
+        assert_parity(y, orc.cf_csr(row, col, val, x), orc.abs_csr(row, col, val, x), 1e-8, what=f"{fmt} f32lo all")
+
+
+def test_precision_forms_rejected_elsewhere(env):
+    torch, D, F, orc = env
+    from int_spmv_b200 import IntSpmvError
+    g = load_golden("random257_empty")
+    csr = F.CSR(g["row"], g["col"], g["val"])
+    with pytest.raises(IntSpmvError):
+        make_plan(F, D, csr, g["x"], "K1P", col="d16")
+    with pytest.raises(IntSpmvError):
+        make_plan(F, D, csr, g["x"], "NOC4", val="f32lo", kernel="ldg")
+    with pytest.raises(IntSpmvError):
+        make_plan(F, D, csr, g["x"], "CSR", col="d16", kernel="rows")
