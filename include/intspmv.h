@@ -194,6 +194,25 @@ int ispmv_dev_int_axt_noc(UIN tileNum, UIN tileHeight, const FPT *ax, const UIN 
 int ispmv_dev_int_axt_com_h1(UIN bn, UIN bs, UIN log, UIN thw, UIN tn, UIN lenAX, UIN lenRWP,
                              const FPT *ax, const UIN *rwp, FPT *y, void *stream);
 
+/* K1 SpMV in original row order, y[permi[i]] = (chunk-order product)[i],
+ * that allocates nothing.  No counterpart in the reference (whose int_k1
+ * writes a caller-provided result array that orderArrayK1 then reorders).
+ * For callers that cannot call cudaMalloc - a solver loop whose memory is
+ * fixed before it starts, or a host that gives the library no allocator -
+ * the chunk-order intermediate lives in a static device array of
+ * ISPMV_K1_NOALLOC_MAX_ROWS doubles (8 MiB), held by every GPU that loads
+ * the library until the process exits.  Arrays are those of str_matK1 on
+ * the device; vec and y have nrows entries; chunkNum = ceil(nrows / 8).
+ * More rows than the maximum is rejected with ISPMV_ERR_ARG.  The first call
+ * on each device looks up the array's device address (cudaGetSymbolAddress),
+ * so make that first call before any stream capture.  Calls share the
+ * array: calls that overlap on the GPU (concurrent streams, or several host
+ * threads) race and must be serialised by the caller.  Nothing needs
+ * clearing between calls: every call writes the part of the array it reads. */
+#define ISPMV_K1_NOALLOC_MAX_ROWS (1u << 20)
+int ispmv_dev_k1_spmv_noalloc(UIN nrows, UIN chunkNum, const FPT *val, const UIN *col, const UIN *chp,
+                              const UIN *nmc, const UIN *permi, const FPT *vec, FPT *y, void *stream);
+
 /* ---------------------------------------------------------------------------
  * Layer 2b: the reference's kernels by name on HOST pointers.  Each call
  * copies its inputs to the current GPU, runs the ispmv_dev_* kernel and

@@ -99,6 +99,7 @@ PROTOTYPES: dict[str, tuple] = {
     "ispmv_dev_int_axt_noc_h1": (C.c_int, [UIN, VP, VP, VP, VP]),
     "ispmv_dev_int_axt_noc": (C.c_int, [UIN, UIN, VP, VP, VP, VP]),
     "ispmv_dev_int_axt_com_h1": (C.c_int, [UIN, UIN, UIN, UIN, UIN, UIN, UIN, VP, VP, VP, VP]),
+    "ispmv_dev_k1_spmv_noalloc": (C.c_int, [UIN, UIN, VP, VP, VP, VP, VP, VP, VP, VP]),
     # the reference's kernels by name, on host pointers
     "cf_CSR": (None, [StrMatCSR, P_FPT, P_FPT]),
     "int_axc": (None, [UIN, UIN, P_FPT, P_UIN, P_FPT]),

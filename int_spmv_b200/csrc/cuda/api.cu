@@ -17,6 +17,11 @@ int cuda_status(cudaError_t e, const char *where) {
   return e == cudaErrorMemoryAllocation ? ISPMV_ERR_OOM : ISPMV_ERR_CUDA;
 }
 
+int fail(int status, const char *text) {
+  std::snprintf(g_last_error, sizeof g_last_error, "%s", text);
+  return status;
+}
+
 void count_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 int check_launch(const char *where) {

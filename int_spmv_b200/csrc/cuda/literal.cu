@@ -282,6 +282,56 @@ ISPMV_API int ispmv_dev_int_axt_com_h1(UIN bn, UIN bs, UIN log, UIN thw, UIN tn,
 }
 
 // ---------------------------------------------------------------------------
+// K1 product in original row order that allocates nothing.  The chunk-order
+// result of the K1 kernel (the `res` array int_k1 hands to orderArrayK1)
+// lives in this file-scope device array instead of caller or library
+// allocations; every GPU that loads the library holds it (8 MiB) until exit.
+static __device__ __align__(256) double g_k1_rows[ISPMV_K1_NOALLOC_MAX_ROWS];
+
+namespace {
+std::mutex g_k1_rows_mu;
+double *g_k1_rows_addr[64] = {nullptr};  // the array's device address, per device
+
+// The array's address on the current device, looked up once per device with
+// that device current (the host-side symbol is not a device address).
+int k1_rows_scratch(double **out) {
+  int dev = 0;
+  ISPMV_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(ISPMV_ERR_UNSUPPORTED, "ispmv_dev_k1_spmv_noalloc: device index >= 64");
+  std::lock_guard<std::mutex> g(g_k1_rows_mu);
+  if (!g_k1_rows_addr[dev]) {
+    void *addr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&addr, g_k1_rows);
+    if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(g_k1_rows)");
+    g_k1_rows_addr[dev] = static_cast<double *>(addr);
+  }
+  *out = g_k1_rows_addr[dev];
+  return ISPMV_OK;
+}
+}  // namespace
+
+ISPMV_API int ispmv_dev_k1_spmv_noalloc(UIN nrows, UIN chunkNum, const FPT *val, const UIN *col, const UIN *chp,
+                                        const UIN *nmc, const UIN *permi, const FPT *vec, FPT *y, void *stream) {
+  if (nrows == 0) return ISPMV_OK;
+  if (!chp || !nmc || !permi || !vec || !y) return ISPMV_ERR_ARG;
+  if ((uint64_t)chunkNum * 8 < nrows || (uint64_t)chunkNum * 8 >= (uint64_t)nrows + 8)
+    return fail(ISPMV_ERR_ARG, "ispmv_dev_k1_spmv_noalloc: chunkNum must be ceil(nrows / 8)");
+  if ((uint64_t)chunkNum * 8 > ISPMV_K1_NOALLOC_MAX_ROWS)
+    return fail(ISPMV_ERR_ARG, "ispmv_dev_k1_spmv_noalloc: more than ISPMV_K1_NOALLOC_MAX_ROWS (1048576) rows");
+  double *res = nullptr;
+  int st = k1_rows_scratch(&res);
+  if (st) return st;
+  // the K1 kernel writes all chunkNum*8 entries of res before the reorder
+  // reads any, so nothing left by an earlier call is ever read
+  lit::k_k1<false><<<lit::blocks_for((size_t)chunkNum * 8), lit::TPB, 0, as_stream(stream)>>>(
+      chunkNum, 0xFF, val, col, chp, nmc, nullptr, vec, res);
+  st = check_launch("ispmv_dev_k1_spmv_noalloc (chunks)");
+  if (st) return st;
+  lit::k_order<<<lit::blocks_for(nrows), lit::TPB, 0, as_stream(stream)>>>(nrows, permi, res, y);
+  return check_launch("ispmv_dev_k1_spmv_noalloc (reorder)");
+}
+
+// ---------------------------------------------------------------------------
 // Host-pointer forms with the reference's names.  A small grow-only pool of
 // device buffers per process keeps repeated calls from re-allocating.
 namespace {
