@@ -156,6 +156,12 @@ str_formatData getFormatDataAXT(const UIN ompNT, const UIN bs, const UIN thw, co
 int ispmv_build_axc_cols(UIN ompNT, const str_matCSR *csr, const str_matAXC *axc, UIN **axi);
 int ispmv_build_axt_cols(UIN ompNT, const str_matCSR *csr, const str_matAXT *axt, UIN **axi);
 
+/* Block-diagonal CSR of `count` square matrices (no reference counterpart:
+ * the batched path).  Matrix m's rows and columns start at off[m]; off has
+ * count+1 entries.  Arrays are malloc'd (ispmv_csr_free); rl and the
+ * statistics are filled. */
+int ispmv_csr_blockdiag(UIN count, const str_matCSR *mats, str_matCSR *out, UIN *off);
+
 /* Frees the arrays a builder allocated and zeroes the struct. */
 void ispmv_free_axc(str_matAXC *m);
 void ispmv_free_k1(str_matK1 *m);
@@ -256,6 +262,7 @@ typedef struct ispmv_plan_s *ispmv_plan;
 #define ISPMV_KERNEL_LDG 1   /* slot-stream kernel, plain loads, register prefetch */
 #define ISPMV_KERNEL_TMA 2   /* slot-stream kernel, 1D bulk copies (cp.async.bulk) into shared memory */
 #define ISPMV_KERNEL_ROWS 3  /* row-parallel kernel (CSR: lanes per row; AXC: 8 lanes per row; K1) */
+#define ISPMV_VARIANT_QUEUE 16 /* slot-stream kernel as a work queue drained by persistent warps */
 
 typedef struct {
   int val_kind;      /* ISPMV_VAL_* */
@@ -265,7 +272,10 @@ typedef struct {
   int units_per_warp;/* work granule of one warp; 0 = library default */
   double lo_tol;     /* F32_LO16: rows whose FP32 rounding error bound exceeds
                         lo_tol relative carry a lo-word; 0 = default 1e-9 */
-  int variant;       /* kernel variant (prefetch depth / register budget); 0 = default */
+  int variant;       /* kernel variant (prefetch depth / register budget); 0 = default;
+                        ISPMV_VARIANT_QUEUE = persistent warps pulling segments
+                        from a device work queue */
+  int rhs_block;     /* SpMM right-hand sides per pass: 8, 16 or 32; 0 = by k */
 } ispmv_plan_opts;
 
 void ispmv_plan_opts_default(ispmv_plan_opts *o);
@@ -285,6 +295,10 @@ int ispmv_plan_destroy(ispmv_plan p);
 
 /* y = A*x + beta*y with device pointers, beta in {0, 1}.  Stream-ordered. */
 int ispmv_plan_spmv(ispmv_plan p, const FPT *x, FPT *y, int beta, void *stream);
+/* The same product as one CUDA-graph launch: the plan captures its kernels
+ * (queue reset, SpMV, row fix-up) for this (x, y, beta) on first use, and
+ * captures again when they change.  Stream-ordered on `stream`. */
+int ispmv_plan_spmv_graph(ispmv_plan p, const FPT *x, FPT *y, int beta, void *stream);
 /* Y = A*X for k right-hand sides, X and Y row-major (n x k), FP64. */
 int ispmv_plan_spmm(ispmv_plan p, UIN k, const FPT *X, FPT *Y, void *stream);
 /* End to end on HOST buffers: copies x in, runs the SpMV, copies y out and
@@ -295,6 +309,19 @@ int ispmv_plan_spmv_host(ispmv_plan p, const FPT *h_x, FPT *h_y, void *stream);
  * wait of a staged kernel gave up (the result is then invalid), else OK.
  * Synchronous (reads a device status word). */
 int ispmv_plan_status(ispmv_plan p);
+
+/* Kernel timing.  With pairs > 0 every ispmv_plan_spmv records a CUDA event
+ * pair on its stream around the product's main kernel (not around the row
+ * fix-up or K1's reorder that follow it), in a ring of `pairs` pairs;
+ * pairs = 0 turns it off.  Graph launches record nothing.
+ * ispmv_plan_kernel_ms returns the summed elapsed time of the recorded pairs
+ * (at most `pairs`, the latest) and how many, then restarts the count; call
+ * it after the stream is synchronised. */
+int ispmv_plan_time_kernels(ispmv_plan p, int pairs);
+int ispmv_plan_kernel_ms(ispmv_plan p, double *total_ms, int *launches);
+/* Name of the main kernel the plan's latest product launched (a static
+ * string, "" before the first product), e.g. "stream_ldg<4,0,5>". */
+const char *ispmv_plan_kernel_name(ispmv_plan p);
 
 /* Plan facts: rows, nonzeros, value slots streamed, bytes of device
  * storage, and the algorithmic bytes of one SpMV:

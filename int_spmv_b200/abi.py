@@ -49,7 +49,7 @@ class StrMatAXT(C.Structure):  # intSpmv_main.c:1114
 
 class PlanOpts(C.Structure):
     _fields_ = [("val_kind", C.c_int), ("col_kind", C.c_int), ("kernel", C.c_int), ("ctas_per_sm", C.c_int),
-                ("units_per_warp", C.c_int), ("lo_tol", C.c_double), ("variant", C.c_int)]
+                ("units_per_warp", C.c_int), ("lo_tol", C.c_double), ("variant", C.c_int), ("rhs_block", C.c_int)]
 
 
 class PlanInfo(C.Structure):
@@ -85,6 +85,7 @@ PROTOTYPES: dict[str, tuple] = {
     "getFormatDataAXT": (StrFormatData, [UIN, UIN, UIN, UIN, C.c_char_p, StrMatCSR, P_FPT, P_AXT]),
     "ispmv_build_axc_cols": (C.c_int, [UIN, P_CSR, P_AXC, P_P_UIN]),
     "ispmv_build_axt_cols": (C.c_int, [UIN, P_CSR, P_AXT, P_P_UIN]),
+    "ispmv_csr_blockdiag": (C.c_int, [UIN, P_CSR, P_CSR, P_UIN]),
     "ispmv_free_axc": (None, [P_AXC]),
     "ispmv_free_k1": (None, [P_K1]),
     "ispmv_free_axt": (None, [P_AXT]),
@@ -117,10 +118,14 @@ PROTOTYPES: dict[str, tuple] = {
     "ispmv_plan_axt": (C.c_int, [P_CSR, P_AXT, P_UIN, P_OPTS, P_PLAN]),
     "ispmv_plan_destroy": (C.c_int, [VP]),
     "ispmv_plan_spmv": (C.c_int, [VP, VP, VP, C.c_int, VP]),
+    "ispmv_plan_spmv_graph": (C.c_int, [VP, VP, VP, C.c_int, VP]),
     "ispmv_plan_spmm": (C.c_int, [VP, UIN, VP, VP, VP]),
     "ispmv_plan_spmv_host": (C.c_int, [VP, VP, VP, VP]),
     "ispmv_plan_get_info": (C.c_int, [VP, C.POINTER(PlanInfo)]),
     "ispmv_plan_status": (C.c_int, [VP]),
+    "ispmv_plan_time_kernels": (C.c_int, [VP, C.c_int]),
+    "ispmv_plan_kernel_ms": (C.c_int, [VP, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+    "ispmv_plan_kernel_name": (C.c_char_p, [VP]),
     # library facts
     "ispmv_version": (C.c_char_p, []),
     "ispmv_status_string": (C.c_char_p, [C.c_int]),
@@ -133,3 +138,4 @@ OK, ERR_ARG, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_OVERFLOW = ran
 VAL_F64, VAL_F32, VAL_F32_LO16 = 0, 1, 2
 COL_U32, COL_D16 = 0, 1
 KERNEL_AUTO, KERNEL_LDG, KERNEL_TMA, KERNEL_ROWS = 0, 1, 2, 3
+VARIANT_QUEUE = 16

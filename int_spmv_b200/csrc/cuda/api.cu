@@ -8,6 +8,7 @@
 namespace ispmv {
 namespace {
 thread_local char g_last_error[256] = "";
+thread_local const char *g_last_launch = "";
 std::atomic<unsigned long long> g_launches{0};
 int g_sms[64] = {0};
 }  // namespace
@@ -26,9 +27,12 @@ void count_launch(unsigned n) { g_launches.fetch_add(n, std::memory_order_relaxe
 
 int check_launch(const char *where) {
   count_launch();
+  g_last_launch = where;
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? ISPMV_OK : cuda_status(e, where);
 }
+
+const char *last_launch() { return g_last_launch; }
 
 int sm_count() {
   int dev = 0;

@@ -19,6 +19,8 @@ int cuda_status(cudaError_t e, const char *where);
 void count_launch(unsigned n = 1);
 // Checks the launch just made on the calling thread.
 int check_launch(const char *where);
+// Name given to the calling thread's latest check_launch (a static string).
+const char *last_launch();
 // Records a library error text for ispmv_last_error() and returns `status`.
 int fail(int status, const char *text);
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }

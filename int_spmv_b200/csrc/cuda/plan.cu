@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "plan_tma.cuh"
+#include "spmm.cuh"
 #include "sss.cuh"
 
 using namespace ispmv;
@@ -54,8 +55,23 @@ struct ispmv_plan_s {
   double lo_frac = 0.0;   // fraction of slots carrying a lo-word
   size_t esc_batches = 0; // D16 batches kept as u32 columns
   FPT *hx = nullptr, *hy = nullptr;  // device staging of ispmv_plan_spmv_host
+  unsigned long long *queue = nullptr;  // work-queue counter (variant ISPMV_VARIANT_QUEUE)
+  cudaStream_t cap_stream = nullptr;    // private stream for graph capture
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  const FPT *g_x = nullptr;
+  FPT *g_y = nullptr;
+  int g_beta = -1;
+  UIN *mm_row = nullptr;             // SpMM records (allocated on first use)
+  double *mm_sum = nullptr;
+  size_t mm_cap = 0;                 // doubles in mm_sum
   std::vector<void *> owned;
   ispmv_plan_info info{};
+  std::vector<cudaEvent_t> tev;      // kernel timing: event pairs around the main kernel (a ring)
+  size_t tcap = 0;                   // pairs in the ring (0: timing off)
+  size_t tcount = 0;                 // pairs recorded since the last read
+  bool capturing = false;            // inside graph capture: no timing events
+  const char *kname = "";            // main kernel of the latest product (a static string)
 };
 
 namespace {
@@ -182,6 +198,7 @@ int alloc_records(ispmv_plan_s *p) {
   TRY(dev_alloc(p, std::max<size_t>(1, 2 * p->nseg), &p->rec_sum));
   TRY(dev_alloc(p, 1, &p->status));
   ISPMV_TRY(cudaMemset(p->status, 0, sizeof(int)));
+  TRY(dev_alloc(p, 1, &p->queue));
   return ISPMV_OK;
 }
 
@@ -198,6 +215,10 @@ bool xw_variant(int v, XwCfg *c) {
     case 9: *c = {16, 8192, 1024}; return true;
     case 10: *c = {8, 2048, 1024}; return true;
     case 11: *c = {16, 6144, 2048}; return true;
+    case 17: *c = {16, 4096, 1024}; return true;  // lean gathers (stream_xw2)
+    case 18: *c = {16, 8192, 2048}; return true;
+    case 19: *c = {8, 4096, 2048}; return true;
+    case 20: *c = {16, 12288, 2048}; return true;
     default: return false;
   }
 }
@@ -361,6 +382,10 @@ ISPMV_API void ispmv_plan_opts_default(ispmv_plan_opts *o) {
 
 ISPMV_API int ispmv_plan_destroy(ispmv_plan p) {
   if (!p) return ISPMV_OK;
+  for (cudaEvent_t e : p->tev) cudaEventDestroy(e);
+  if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
   for (void *q : p->owned) cudaFree(q);
   delete p;
   return ISPMV_OK;
@@ -570,6 +595,17 @@ int launch_staged(K kernel, size_t smem, size_t nseg, int ctas_per_sm, cudaStrea
   return check_launch(what);
 }
 
+template <int W, typename K>
+int launch_staged_w(K kernel, size_t smem, size_t nseg, int ctas_per_sm, cudaStream_t s, const char *what,
+                    void **args) {
+  const size_t want = (nseg + W - 1) / W;
+  const size_t cap = (size_t)sm_count() * (size_t)ctas_per_sm;
+  const unsigned g = (unsigned)std::max<size_t>(1, std::min(want, cap));
+  ISPMV_TRY(cudaFuncSetAttribute((const void *)kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  ISPMV_TRY(cudaLaunchKernel((const void *)kernel, dim3(g), dim3(W * 32), args, smem, s));
+  return check_launch(what);
+}
+
 template <typename VT>
 int run_stream(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
   const VT *val = static_cast<const VT *>(p->val);
@@ -587,6 +623,31 @@ int run_stream(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
     return check_launch("stream_narrow");
   }
   XwCfg xc;
+  if (p->opts.kernel == ISPMV_KERNEL_LDG && p->opts.variant >= 17 && xw_variant(p->opts.variant, &xc)) {
+    const size_t smem = (size_t)xc.cap * sizeof(double);
+    const unsigned g = (unsigned)((nseg + xc.warps - 1) / xc.warps);
+    const int nw = std::max(1, p->xw.nwin);
+#define ISPMV_XW2(NW, W)                                                                                       \
+  do {                                                                                                          \
+    ISPMV_TRY(cudaFuncSetAttribute((const void *)sss::stream_xw2<VT, NW, W>,                                    \
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));                    \
+    sss::stream_xw2<VT, NW, W><<<g, W * 32, smem, s>>>(nslots, spad, sslots, nseg, val, col, heads, segh, p->xw, \
+                                                       x, o);                                                   \
+    nm = "stream_xw2<" #NW "," #W ">";                                                                          \
+  } while (0)
+    const char *nm = "stream_xw2";
+    if (xc.warps == 16) {
+      if (nw == 1) ISPMV_XW2(1, 16);
+      else if (nw == 2) ISPMV_XW2(2, 16);
+      else ISPMV_XW2(3, 16);
+    } else {
+      if (nw == 1) ISPMV_XW2(1, 8);
+      else if (nw == 2) ISPMV_XW2(2, 8);
+      else ISPMV_XW2(3, 8);
+    }
+#undef ISPMV_XW2
+    return check_launch(nm);
+  }
   if (p->opts.kernel == ISPMV_KERNEL_LDG && xw_variant(p->opts.variant, &xc)) {
     const size_t smem = (size_t)xc.cap * sizeof(double);
     const unsigned g = (unsigned)((nseg + xc.warps - 1) / xc.warps);
@@ -604,27 +665,60 @@ int run_stream(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
   if (p->opts.kernel == ISPMV_KERNEL_TMA) {
     int *status = p->status;
     void *args[] = {&nslots, &spad, &sslots, &nseg, &val, &col, &heads, &segh, (void *)&x, &o, &status};
-    return launch_staged(sss::stream_tma<VT, TW, TS>, sss::smem_bytes<TW, TS, VT>(), nseg, p->opts.ctas_per_sm, s,
-                         "stream_tma", args);
+    const int cps = p->opts.ctas_per_sm;
+    // variants: (warps per CTA, stages per warp, slots per stage); CTAs per SM from shared memory
+    switch (p->opts.variant) {
+      case 1:
+        return launch_staged_w<8>(sss::stream_tma<VT, 8, 3, 256>, sss::smem_bytes<8, 3, VT, 256>(), nseg,
+                                  cps ? cps : 3, s, "stream_tma<8,3,256>", args);
+      case 2:
+        return launch_staged_w<16>(sss::stream_tma<VT, 16, 2, 128>, sss::smem_bytes<16, 2, VT, 128>(), nseg,
+                                   cps ? cps : 4, s, "stream_tma<16,2,128>", args);
+      case 3:
+        return launch_staged_w<4>(sss::stream_tma<VT, 4, 4, 512>, sss::smem_bytes<4, 4, VT, 512>(), nseg,
+                                  cps ? cps : 2, s, "stream_tma<4,4,512>", args);
+      default:
+        return launch_staged_w<8>(sss::stream_tma<VT, 8, 2, 256>, sss::smem_bytes<8, 2, VT, 256>(), nseg,
+                                  cps ? cps : 4, s, "stream_tma<8,2,256>", args);
+    }
+  }
+  if (p->opts.variant == ISPMV_VARIANT_QUEUE) {
+    ISPMV_TRY(cudaMemsetAsync(p->queue, 0, sizeof(unsigned long long), s));
+    const size_t warps = std::min<size_t>(nseg, (size_t)sm_count() * 6 * 8);
+    const unsigned gq = (unsigned)std::max<size_t>(1, (warps + 7) / 8);
+    sss::stream_queue<VT><<<gq, 256, 0, s>>>(nslots, spad, sslots, nseg, val, col, heads, segh, x, p->queue, o);
+    return check_launch("stream_queue");
   }
   const unsigned g = (unsigned)((nseg * 32 + 255) / 256);
   // variants: slots per lane x prefetch depth (batches in flight) x CTAs per
-  // SM the register budget allows; variant 0 is the default
+  // SM the register budget allows; the default (variant 0) is (4, 0, 5)
+  const char *nm = "stream_ldg";
 #define ISPMV_SSS(SPL, PD, MINB)                                                                              \
   sss::stream_ldg<VT, SPL, PD, MINB><<<g, 256, 0, s>>>(nslots, spad, sslots, nseg, val, col, heads, segh, x, o); \
+  nm = "stream_ldg<" #SPL "," #PD "," #MINB ">";                                                                \
+  break
+#define ISPMV_SSS_PF(SPL, PD, MINB, PF)                                                              \
+  sss::stream_ldg<VT, SPL, PD, MINB, PF><<<g, 256, 0, s>>>(nslots, spad, sslots, nseg, val, col, heads, segh, x, \
+                                                           o);                                                   \
+  nm = "stream_ldg<" #SPL "," #PD "," #MINB ",pf" #PF ">";                                                      \
   break
   switch (p->opts.variant) {
     case 1: ISPMV_SSS(4, 1, 4);
-    case 2: ISPMV_SSS(4, 0, 5);
+    case 2: ISPMV_SSS(4, 0, 6);
     case 3: ISPMV_SSS(2, 1, 6);
     case 4: ISPMV_SSS(2, 0, 8);
     case 5: ISPMV_SSS(2, 1, 5);
     case 6: ISPMV_SSS(4, 0, 8);
     case 7: ISPMV_SSS(2, 0, 6);
-    default: ISPMV_SSS(4, 0, 6);
+    case 12: ISPMV_SSS_PF(4, 0, 6, 2);
+    case 13: ISPMV_SSS_PF(4, 0, 6, 4);
+    case 14: ISPMV_SSS_PF(4, 0, 6, 8);
+    case 15: ISPMV_SSS_PF(4, 0, 5, 4);
+    default: ISPMV_SSS(4, 0, 5);
   }
 #undef ISPMV_SSS
-  return check_launch("stream_ldg");
+#undef ISPMV_SSS_PF
+  return check_launch(nm);
 }
 
 template <typename VT>
@@ -657,8 +751,47 @@ int run_units(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
   return check_launch("noc_hn");
 }
 
+// Kernel timing marks: `which` 0 before the main kernel of a product, 1 after it.
+int tmark(ispmv_plan_s *p, cudaStream_t s, int which) {
+  if (!p->tcap || p->capturing) return ISPMV_OK;
+  const size_t i = p->tcount % p->tcap;
+  ISPMV_TRY(cudaEventRecord(p->tev[2 * i + which], s));
+  if (which) p->tcount++;
+  return ISPMV_OK;
+}
+
+template <typename VT>
+int run_main(ispmv_plan_s *p, const FPT *x, FPT *y, int beta, cudaStream_t s);
+
 template <typename VT>
 int run(ispmv_plan_s *p, const FPT *x, FPT *y, int beta, cudaStream_t s) {
+  TRY(tmark(p, s, 0));
+  const int st = run_main<VT>(p, x, y, beta, s);
+  if (st) return st;
+  p->kname = last_launch();
+  // the kernels after the main one (the row fix-up, K1's reorder)
+  if (p->path == P_STREAM || p->path == P_UNITS) {
+    TRY(tmark(p, s, 1));
+    const size_t nrec = p->slots ? 2 * p->nseg : 0;
+    const size_t work = std::max(nrec, p->nempty);
+    if (work) {
+      seg::fixup<<<(unsigned)((work + 255) / 256), 256, 0, s>>>(nrec, p->rec_row, p->rec_sum, p->rowmap, p->empty,
+                                                                p->nempty, y, beta);
+      return check_launch("fixup");
+    }
+    return ISPMV_OK;
+  }
+  if (p->path == P_K1 && p->fmt != F_K1P) {
+    TRY(tmark(p, s, 1));
+    pk::k1_order<<<(unsigned)((p->n + 255) / 256), 256, 0, s>>>(p->n, p->permi, p->res, y, beta);
+    return check_launch("k1_order");
+  }
+  return tmark(p, s, 1);
+}
+
+// The main kernel of one product.
+template <typename VT>
+int run_main(ispmv_plan_s *p, const FPT *x, FPT *y, int beta, cudaStream_t s) {
   const VT *val = static_cast<const VT *>(p->val);
   switch (p->path) {
     case P_ROWS: {
@@ -687,21 +820,12 @@ int run(ispmv_plan_s *p, const FPT *x, FPT *y, int beta, cudaStream_t s) {
       }
       pk::k1_chunks<VT, false><<<g, pk::TPB, 0, s>>>(p->n, p->chunkNum, p->chp, p->nmc, p->permi, p->col, val, x,
                                                      p->res, beta);
-      TRY(check_launch("k1_chunks"));
-      pk::k1_order<<<(unsigned)((p->n + 255) / 256), 256, 0, s>>>(p->n, p->permi, p->res, y, beta);
-      return check_launch("k1_order");
+      return check_launch("k1_chunks");
     }
     case P_STREAM:
     case P_UNITS: {
       seg::Out o{y, p->rowmap, p->rec_row, p->rec_sum, beta};
       if (p->slots) TRY(p->path == P_STREAM ? run_stream<VT>(p, x, o, s) : run_units<VT>(p, x, o, s));
-      const size_t nrec = p->slots ? 2 * p->nseg : 0;
-      const size_t work = std::max(nrec, p->nempty);
-      if (work) {
-        seg::fixup<<<(unsigned)((work + 255) / 256), 256, 0, s>>>(nrec, p->rec_row, p->rec_sum, p->rowmap, p->empty,
-                                                                  p->nempty, y, beta);
-        return check_launch("fixup");
-      }
       return ISPMV_OK;
     }
     default:
@@ -717,6 +841,69 @@ ISPMV_API int ispmv_plan_spmv(ispmv_plan p, const FPT *x, FPT *y, int beta, void
   if (p->opts.val_kind == ISPMV_VAL_F64) return run<double>(p, x, y, beta, s);
   return run<float>(p, x, y, beta, s);
 }
+
+ISPMV_API int ispmv_plan_spmv_graph(ispmv_plan p, const FPT *x, FPT *y, int beta, void *stream) {
+  if (!p || !x || !y || (beta != 0 && beta != 1)) return ISPMV_ERR_ARG;
+  if (!p->graph_exec || p->g_x != x || p->g_y != y || p->g_beta != beta) {
+    if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
+    if (p->graph) cudaGraphDestroy(p->graph);
+    p->graph_exec = nullptr;
+    p->graph = nullptr;
+    if (!p->cap_stream) ISPMV_TRY(cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking));
+    ISPMV_TRY(cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal));
+    p->capturing = true;
+    const int st = p->opts.val_kind == ISPMV_VAL_F64 ? run<double>(p, x, y, beta, p->cap_stream)
+                                                     : run<float>(p, x, y, beta, p->cap_stream);
+    p->capturing = false;
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(p->cap_stream, &g);
+    if (st) {
+      if (g) cudaGraphDestroy(g);
+      return st;
+    }
+    if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture");
+    p->graph = g;
+    ISPMV_TRY(cudaGraphInstantiate(&p->graph_exec, p->graph, 0));
+    p->g_x = x;
+    p->g_y = y;
+    p->g_beta = beta;
+  }
+  ISPMV_TRY(cudaGraphLaunch(p->graph_exec, as_stream(stream)));
+  count_launch();
+  return ISPMV_OK;
+}
+
+ISPMV_API int ispmv_plan_time_kernels(ispmv_plan p, int pairs) {
+  if (!p || pairs < 0) return ISPMV_ERR_ARG;
+  for (cudaEvent_t e : p->tev) cudaEventDestroy(e);
+  p->tev.clear();
+  p->tcap = 0;
+  p->tcount = 0;
+  for (int i = 0; i < 2 * pairs; i++) {
+    cudaEvent_t e;
+    ISPMV_TRY(cudaEventCreate(&e));
+    p->tev.push_back(e);
+  }
+  p->tcap = (size_t)pairs;
+  return ISPMV_OK;
+}
+
+ISPMV_API int ispmv_plan_kernel_ms(ispmv_plan p, double *total_ms, int *launches) {
+  if (!p || !total_ms || !launches) return ISPMV_ERR_ARG;
+  const size_t m = std::min(p->tcount, p->tcap);
+  double sum = 0.0;
+  for (size_t i = 0; i < m; i++) {
+    float ms = 0.f;
+    ISPMV_TRY(cudaEventElapsedTime(&ms, p->tev[2 * i], p->tev[2 * i + 1]));
+    sum += ms;
+  }
+  *total_ms = sum;
+  *launches = (int)m;
+  p->tcount = 0;
+  return ISPMV_OK;
+}
+
+ISPMV_API const char *ispmv_plan_kernel_name(ispmv_plan p) { return p ? p->kname : ""; }
 
 ISPMV_API int ispmv_plan_status(ispmv_plan p) {
   if (!p) return ISPMV_ERR_ARG;
@@ -740,7 +927,52 @@ ISPMV_API int ispmv_plan_spmv_host(ispmv_plan p, const FPT *h_x, FPT *h_y, void 
   return ispmv_plan_status(p);
 }
 
+namespace {
+template <int G, typename VT>
+int spmm_blocks(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
+  constexpr int NG = 32 / G;
+  const size_t nparts = p->nseg * NG, nrec = 2 * nparts;
+  if (!p->mm_row) TRY(dev_alloc(p, std::max<size_t>(1, nrec), &p->mm_row));
+  if (p->mm_cap < nrec * G) {
+    TRY(dev_alloc(p, std::max<size_t>(1, nrec * G), &p->mm_sum));
+    p->mm_cap = nrec * G;
+  }
+  const VT *val = static_cast<const VT *>(p->val);
+  for (UIN j0 = 0; j0 < k; j0 += G) {
+    mm::Out o{Y, p->rowmap, p->mm_row, p->mm_sum, k, j0, std::min<UIN>(G, k - j0)};
+    const unsigned g = (unsigned)((p->nseg * 32 + 255) / 256);
+    mm::stream_spmm<G, VT><<<g, 256, 0, s>>>(p->slots, p->slots_pad, p->seg_slots, p->nseg, val, p->col, p->heads,
+                                             p->segh, X, o);
+    TRY(check_launch("stream_spmm"));
+    const size_t work = std::max(nrec, p->nempty) * G;
+    mm::spmm_fixup<G><<<(unsigned)((work + 255) / 256), 256, 0, s>>>(nrec, p->mm_row, p->mm_sum, p->empty,
+                                                                     p->nempty, o);
+    TRY(check_launch("spmm_fixup"));
+  }
+  return ISPMV_OK;
+}
+
+template <typename VT>
+int spmm_run(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
+  int g = p->opts.rhs_block;
+  if (g != 8 && g != 16 && g != 32) g = k <= 8 ? 8 : k <= 16 ? 16 : 32;
+  if (g == 8) return spmm_blocks<8, VT>(p, k, X, Y, s);
+  if (g == 16) return spmm_blocks<16, VT>(p, k, X, Y, s);
+  return spmm_blocks<32, VT>(p, k, X, Y, s);
+}
+}  // namespace
+
+// Y = A X for k right-hand sides (row-major n x k): the slot-stream plans
+// (AXT COM, AXT tileH=1, AXC and CSR built with the stream kernels).
 ISPMV_API int ispmv_plan_spmm(ispmv_plan p, UIN k, const FPT *X, FPT *Y, void *stream) {
-  (void)p; (void)k; (void)X; (void)Y; (void)stream;
-  return ISPMV_ERR_UNSUPPORTED;
+  if (!p || !X || !Y || k == 0) return ISPMV_ERR_ARG;
+  if (p->path != P_STREAM || narrow_kinds(p))
+    return fail(ISPMV_ERR_UNSUPPORTED, "ispmv_plan_spmm: needs a slot-stream plan with u32 columns");
+  cudaStream_t s = as_stream(stream);
+  if (!p->slots) {  // every row empty
+    ISPMV_TRY(cudaMemsetAsync(Y, 0, (size_t)p->n * k * sizeof(FPT), s));
+    return ISPMV_OK;
+  }
+  if (p->opts.val_kind == ISPMV_VAL_F64) return spmm_run<double>(p, k, X, Y, s);
+  return spmm_run<float>(p, k, X, Y, s);
 }

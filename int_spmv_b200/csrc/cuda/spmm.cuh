@@ -1,0 +1,124 @@
+// spmm.cuh - multi-RHS SpMM on the slot stream: Y = A X, X and Y row-major
+// n x k (FP64), one plan's slot stream read once for all k right-hand sides.
+//
+// A warp splits into 32/G groups of G lanes; lane j of a group owns column
+// j0 + j of the current column block (G = 8, 16 or 32 columns).  Each group
+// walks its own contiguous part of the warp's segment slot by slot: 8 slots'
+// values and columns are loaded per step (one per lane, coalesced) and
+// broadcast with shuffles, each lane reads X[col*k + j0 + j] (the group reads
+// a contiguous row piece of X) and accumulates.  Row starts come from the
+// stream's bitmap; a row that ends inside the group's part is written to Y
+// directly, the runs open at the part's two ends become G-wide records that
+// spmm_fixup adds per row.  Deterministic, no atomics.
+#pragma once
+#include "sss.cuh"
+
+namespace ispmv {
+namespace mm {
+
+struct Out {
+  FPT *Y;
+  const UIN *rowmap;
+  UIN *rec_row;     // 2 per part
+  double *rec_sum;  // 2 * G per part
+  UIN k, j0, kb;    // row stride, first column of the block, columns in the block
+};
+
+__device__ __forceinline__ UIN real_row(const Out &o, UIN r) { return o.rowmap ? o.rowmap[r] : r; }
+
+template <int G, typename VT>
+__global__ void __launch_bounds__(256) stream_spmm(size_t nslots, size_t nslots_pad, size_t seg_slots, size_t nseg,
+                                                   const VT *__restrict__ val, const UIN *__restrict__ col,
+                                                   const UIN *__restrict__ heads, const UIN *__restrict__ segh,
+                                                   const FPT *__restrict__ X, Out o) {
+  constexpr int NG = 32 / G;  // groups per warp = parts per segment
+  const unsigned lane = threadIdx.x & 31u, grp = lane / G, j = lane % G;
+  const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (grp * G));
+  const size_t segid = ((size_t)blockIdx.x * 256 + threadIdx.x) >> 5;
+  if (segid >= nseg) return;
+  const size_t s0 = segid * seg_slots;
+  const size_t seg_end = min(s0 + seg_slots, nslots_pad);
+  const size_t part = (seg_end - s0) / NG;  // a multiple of 32
+  const size_t a = s0 + grp * part, b = a + part;
+  const size_t pid = segid * NG + grp;
+  // compressed row of the run open at slot a: starts before a, minus one
+  UIN cr = segh[segid];
+  for (size_t w = s0 >> 5; w < (a >> 5); w++) cr += __popc(__ldg(heads + w));
+  const bool a_head = (__ldg(heads + (a >> 5)) & 1u) != 0;  // a is 32-aligned
+  const UIN row_a = a_head ? NO_ROW : cr - 1u;
+  UIN row = cr - 1u;  // current run's row (advanced at each start)
+  bool have = !a_head;  // the current run has slots in this part
+  double acc = 0.0;
+  const bool live_col = j < o.kb;
+  const size_t xoff = o.j0 + j;
+  if (j == 0) {
+    o.rec_row[2 * pid] = NO_ROW;
+    o.rec_row[2 * pid + 1] = NO_ROW;
+  }
+  if (live_col) {
+    o.rec_sum[(2 * pid) * G + j] = 0.0;
+    o.rec_sum[(2 * pid + 1) * G + j] = 0.0;
+  }
+  for (size_t c0 = a; c0 < b; c0 += G) {
+    // one slot per lane of the group, broadcast below
+    const size_t my = c0 + j;
+    const VT mv = val[my];
+    const UIN mc = col[my];
+    const UIN hw = __ldg(heads + (c0 >> 5));
+#pragma unroll 4
+    for (int i = 0; i < G; i++) {
+      const size_t s = c0 + i;
+      const VT v = __shfl_sync(gmask, mv, grp * G + i);
+      const UIN c = __shfl_sync(gmask, mc, grp * G + i);
+      if ((hw >> ((s & 31u))) & 1u) {  // a row starts at s: the current run ends
+        if (have && live_col) {
+          if (row == row_a) o.rec_sum[(2 * pid) * G + j] = acc;
+          else {
+            const UIN rr = real_row(o, row);
+            o.Y[(size_t)rr * o.k + xoff] = acc;
+          }
+        }
+        if (have && row == row_a && j == 0) o.rec_row[2 * pid] = row;
+        row++;
+        acc = 0.0;
+        have = true;
+      }
+      if (live_col && s < nslots) acc = fma((double)v, __ldg(X + (size_t)c * o.k + xoff), acc);
+    }
+  }
+  // the run open at the part's end
+  if (have) {
+    const bool is_a = row == row_a;
+    if (j == 0) o.rec_row[2 * pid + (is_a ? 0 : 1)] = row;
+    if (live_col) o.rec_sum[(2 * pid + (is_a ? 0 : 1)) * G + j] = acc;
+  }
+}
+
+// Record i (of 2 per part) writes its row if it is that row's last record,
+// adding the row's earlier records; rows with no slot get zeros.
+template <int G>
+__global__ void spmm_fixup(size_t nrec, const UIN *__restrict__ rec_row, const double *__restrict__ rec_sum,
+                           const UIN *__restrict__ empty, size_t nempty, Out o) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t i = t / G;
+  const unsigned j = t % G;
+  if (j >= o.kb) return;
+  if (i < nempty) o.Y[(size_t)empty[i] * o.k + o.j0 + j] = 0.0;
+  if (i >= nrec) return;
+  const UIN r = rec_row[i];
+  if (r == NO_ROW) return;
+  size_t q = i + 1;
+  while (q < nrec && rec_row[q] == NO_ROW) q++;
+  if (q < nrec && rec_row[q] == r) return;
+  double total = rec_sum[i * G + j];
+  for (size_t m = i; m-- > 0;) {
+    const UIN rm = rec_row[m];
+    if (rm == NO_ROW) continue;
+    if (rm != r) break;
+    total += rec_sum[m * G + j];
+  }
+  o.Y[(size_t)real_row(o, r) * o.k + o.j0 + j] = total;
+}
+
+}  // namespace mm
+}  // namespace ispmv

@@ -126,6 +126,67 @@ __device__ __forceinline__ void batch(const double (&p)[SPL], const Words<SPL> &
   st.rbase += tot;
 }
 
+__device__ __forceinline__ unsigned lanemask_le() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_le;" : "=r"(m));
+  return m;
+}
+
+// The 4-slot batch without per-slot branches: a lane's leading piece (slots
+// before its first row start) and trailing piece (from its last row start)
+// are masked sums; only lanes holding two or more row starts (rows shorter
+// than 4 slots) take the loop that writes the runs between them.
+template <>
+__device__ __forceinline__ void batch<4>(const double (&p)[4], const Words<4> &hw, Run &st, const seg::Out &o) {
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned q = lane >> 3, sh = 4u * (lane & 7u);
+  const UIN w0 = hw.w.x, w1 = hw.w.y, w2 = hw.w.z, w3 = hw.w.w;
+  const unsigned c0 = __popc(w0), c1 = c0 + __popc(w1), c2 = c1 + __popc(w2), tot = c2 + __popc(w3);
+  const UIN myw = q == 0 ? w0 : q == 1 ? w1 : q == 2 ? w2 : w3;
+  const unsigned before = q == 0 ? 0u : q == 1 ? c0 : q == 2 ? c1 : c2;
+  const unsigned bits = (myw >> sh) & 0xFu;
+  const UIN rb = st.rbase + before + __popc(myw & ((1u << sh) - 1u));  // row of my first start
+  const int first = bits ? __ffs(bits) - 1 : 4;
+  const int last = bits ? 31 - __clz(bits) : 4;
+  double pre = 0.0, run = 0.0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    pre += (k < first) ? p[k] : 0.0;
+    run += (k >= last) ? p[k] : 0.0;
+  }
+  if (__popc(bits) >= 2) {
+    UIN r = rb;
+    double acc = 0.0;
+    bool open = false;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      if ((bits >> k) & 1u) {
+        if (open) emit(o, st, r++, acc);
+        acc = 0.0;
+        open = true;
+      }
+      acc += open ? p[k] : 0.0;
+    }
+  }
+  if (lane == 0 && st.carry) pre += st.csum;
+  const bool f = bits != 0;
+  const unsigned F = __ballot_sync(FULL, f) & lanemask_le();
+  const int start = F ? 31 - __clz(F) : 0;  // my segment's first lane
+  const int reach = (int)lane - start;      // lanes below me in my segment
+  double I = f ? run : pre;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const double u = __shfl_up_sync(FULL, I, d);
+    if (reach >= d) I += u;
+  }
+  double E = __shfl_up_sync(FULL, I, 1);
+  if (lane == 0) E = 0.0;
+  if (f && (lane > 0 || !(bits & 1u) || st.carry)) emit(o, st, rb - 1u, E + pre);
+  st.csum = __shfl_sync(FULL, I, 31);
+  st.carry = true;
+  st.rbase += tot;
+}
+
 __device__ __forceinline__ void finish(const Run &st, const seg::Out &o) {
   if ((threadIdx.x & 31u) != 0) return;
   const UIN crow = st.rbase - 1u;
@@ -215,7 +276,7 @@ struct Slots {
 // Plain-load kernel: one segment per warp, batches of 32*SPL slots, the
 // loads of the next PD batches in flight while the current one gathers x and
 // reduces; MINB CTAs of 256 threads per SM bound the registers.
-template <typename VT, int SPL, int PD, int MINB>
+template <typename VT, int SPL, int PD, int MINB, int PF = 0>
 __global__ void __launch_bounds__(256, MINB) stream_ldg(size_t nslots, size_t nslots_pad, size_t seg_slots,
                                                         size_t nseg, const VT *__restrict__ val,
                                                         const UIN *__restrict__ col, const UIN *__restrict__ heads,
@@ -234,11 +295,21 @@ __global__ void __launch_bounds__(256, MINB) stream_ldg(size_t nslots, size_t ns
 #pragma unroll
   for (int k = 0; k < PD; k++)
     if (k < nbat) buf[k].get(val, col, heads, s0 + (size_t)k * BT, lane);
+  if (PF > 0 && lane == 0) {  // the first PF batches' streams into L2
+    const size_t pb = min((size_t)PF * BT, s1 - s0);
+    tma::prefetch_l2(val + s0, (uint32_t)(pb * sizeof(VT)));
+    tma::prefetch_l2(col + s0, (uint32_t)(pb * 4));
+  }
   for (int j = 0; j < nbat; j += PD + 1) {
 #pragma unroll
     for (int r = 0; r <= PD; r++) {
       const int jj = j + r;
       if (jj >= nbat) break;
+      if (PF > 0 && lane == 0 && jj + PF < nbat) {  // keep PF batches ahead in L2
+        const size_t pb = s0 + (size_t)(jj + PF) * BT;
+        tma::prefetch_l2(val + pb, BT * sizeof(VT));
+        tma::prefetch_l2(col + pb, BT * 4);
+      }
       const int nx = jj + PD;
       Slots<VT, SPL> &cur = buf[r];
       if (PD == 0) cur.get(val, col, heads, s0 + (size_t)jj * BT, lane);
@@ -256,6 +327,47 @@ __global__ void __launch_bounds__(256, MINB) stream_ldg(size_t nslots, size_t ns
     }
   }
   finish(st, o);
+}
+
+// Work-queue form: persistent warps take whole segments from a device
+// counter (reset to 0 before each launch) until none is left, so the
+// segments of many uneven matrices concatenated into one stream (a
+// block-diagonal batch) are shared out dynamically.  The loop ends when the
+// counter passes the segment count; nothing waits.
+template <typename VT>
+__global__ void __launch_bounds__(256, 6) stream_queue(size_t nslots, size_t nslots_pad, size_t seg_slots,
+                                                       size_t nseg, const VT *__restrict__ val,
+                                                       const UIN *__restrict__ col, const UIN *__restrict__ heads,
+                                                       const UIN *__restrict__ segh, const FPT *__restrict__ x,
+                                                       unsigned long long *queue, seg::Out o) {
+  constexpr int SPL = 4, BT = 128;
+  const unsigned lane = threadIdx.x & 31u;
+  for (;;) {
+    unsigned long long next = 0;
+    if (lane == 0) next = atomicAdd(queue, 1ull);
+    const size_t segid = (size_t)__shfl_sync(FULL, next, 0);
+    if (segid >= nseg) break;
+    const size_t s0 = segid * seg_slots;
+    const size_t s1 = min(s0 + seg_slots, nslots_pad);
+    const int nbat = (int)((s1 - s0) / BT);
+    Run st;
+    begin(st, o, segid, segh[segid], __ldg(heads + (s0 >> 5)));
+    for (int j = 0; j < nbat; j++) {
+      Slots<VT, SPL> cur;
+      cur.get(val, col, heads, s0 + (size_t)j * BT, lane);
+      const size_t sl = s0 + (size_t)j * BT + SPL * lane;
+      double p[SPL];
+#pragma unroll
+      for (int k = 0; k < SPL; k++) p[k] = pk::prod<VT>(cur.v[k], ldg(x + cur.c[k]));
+      if (sl + SPL > nslots) {
+#pragma unroll
+        for (int k = 0; k < SPL; k++)
+          if (sl + k >= nslots) p[k] = 0.0;
+      }
+      batch<SPL>(p, cur.h, st, o);
+    }
+    finish(st, o);
+  }
 }
 
 // x windows: up to XW_MAX diagonal bands of x staged in shared memory.
@@ -366,6 +478,89 @@ __global__ void __launch_bounds__(WARPS * 32, 48 / WARPS) stream_xw(size_t nslot
   finish(st, o);
 }
 
+// Lean x-band gathers: NW bands known at compile time, one unsigned compare
+// per band, and one generic-address load that reads shared memory for a
+// column inside a band and global memory (L1/L2) otherwise.
+template <int NW>
+__device__ __forceinline__ double xw_gather(const WinState &w, const double *sx, const FPT *__restrict__ x, UIN c) {
+  const double *src = x + c;
+#pragma unroll
+  for (int k = NW - 1; k >= 0; k--) {
+    const UIN d = c - (UIN)w.lo[k];  // band starts lie in [0, n]: the unsigned difference is exact
+    if (d < w.len[k]) src = sx + w.base[k] + d;
+  }
+  return *src;
+}
+
+template <typename VT, int NW, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, 48 / WARPS) stream_xw2(size_t nslots, size_t nslots_pad,
+                                                                     size_t seg_slots, size_t nseg,
+                                                                     const VT *__restrict__ val,
+                                                                     const UIN *__restrict__ col,
+                                                                     const UIN *__restrict__ heads,
+                                                                     const UIN *__restrict__ segh, XWin xw,
+                                                                     const FPT *__restrict__ x, seg::Out o) {
+  constexpr int SPL = 4, BT = 128;
+  extern __shared__ __align__(16) double sx[];
+  __shared__ WinState sw;
+  const unsigned lane = threadIdx.x & 31u;
+  const size_t seg0 = (size_t)blockIdx.x * WARPS;
+  const size_t segid = seg0 + (threadIdx.x >> 5);
+  if (threadIdx.x == 0) {
+    const size_t segl = min(seg0 + WARPS, nseg);
+    UIN c0 = segh[seg0];
+    c0 = c0 > 0 ? c0 - 1 : 0;
+    UIN c1 = segl < nseg ? segh[segl] : xw.nrows_c;
+    c1 = c1 > 0 ? c1 - 1 : 0;
+    if (c1 >= xw.nrows_c) c1 = xw.nrows_c ? xw.nrows_c - 1 : 0;
+    const long long r0 = xw.rowmap ? xw.rowmap[c0] : c0, r1 = xw.rowmap ? xw.rowmap[c1] : c1;
+    UIN used = 0;
+#pragma unroll
+    for (int k = 0; k < XW_MAX; k++) {
+      long long lo = r0 + xw.off[k] - xw.half[k], hi = r1 + xw.off[k] + xw.half[k] + 1;
+      lo = lo < 0 ? 0 : lo;
+      hi = hi > (long long)xw.n ? (long long)xw.n : hi;
+      long long len = (k < NW && hi > lo) ? hi - lo : 0;
+      if (len > (long long)(xw.cap - used)) len = xw.cap - used;
+      sw.lo[k] = lo;
+      sw.len[k] = (UIN)len;
+      sw.base[k] = used;
+      used += (UIN)len;
+    }
+  }
+  __syncthreads();
+  WinState w;
+#pragma unroll
+  for (int k = 0; k < XW_MAX; k++) {
+    w.lo[k] = sw.lo[k];
+    w.len[k] = sw.len[k];
+    w.base[k] = sw.base[k];
+    for (UIN i = threadIdx.x; i < w.len[k]; i += WARPS * 32) sx[w.base[k] + i] = __ldg(x + w.lo[k] + i);
+  }
+  __syncthreads();
+  if (segid >= nseg) return;
+  const size_t s0 = segid * seg_slots;
+  const size_t s1 = min(s0 + seg_slots, nslots_pad);
+  const int nbat = (int)((s1 - s0) / BT);
+  Run st;
+  begin(st, o, segid, segh[segid], __ldg(heads + (s0 >> 5)));
+  for (int j = 0; j < nbat; j++) {
+    Slots<VT, SPL> cur;
+    cur.get(val, col, heads, s0 + (size_t)j * BT, lane);
+    const size_t sl = s0 + (size_t)j * BT + SPL * lane;
+    double p[SPL];
+#pragma unroll
+    for (int k = 0; k < SPL; k++) p[k] = pk::prod<VT>(cur.v[k], xw_gather<NW>(w, sx, x, cur.c[k]));
+    if (sl + SPL > nslots) {
+#pragma unroll
+      for (int k = 0; k < SPL; k++)
+        if (sl + k >= nslots) p[k] = 0.0;
+    }
+    batch<SPL>(p, cur.h, st, o);
+  }
+  finish(st, o);
+}
+
 // Reduced-byte streams (4 slots per lane, no prefetch, 6 CTAs/SM):
 //   LO   FP32 values plus, in segments whose rows need it, a BF16 residual
 //        lo-word per slot: value = hi + lo, multiplied by x in FP64.
@@ -444,34 +639,37 @@ __global__ void __launch_bounds__(256, 6) stream_narrow(size_t nslots, size_t ns
   finish(st, o);
 }
 
-// Staged kernel: persistent warps, each with a ring of STAGES 512-slot
-// stages filled by 1D bulk copies (values, columns, bitmap).
+// Staged kernel: persistent warps, each with a ring of STAGES stages of
+// SSZ slots filled by 1D bulk copies (values, columns, bitmap).  Streams are
+// padded to SS = 512 slots, so any SSZ dividing 512 fits them.
 constexpr int SS = 512;
 
-template <typename VT>
+template <typename VT, int SSZ>
 constexpr uint32_t stage_bytes() {
-  return SS * sizeof(VT) + SS * 4 + SS / 8;
+  return SSZ * sizeof(VT) + SSZ * 4 + SSZ / 8;
 }
 
-template <int WARPS, int STAGES, typename VT>
+template <int WARPS, int STAGES, typename VT, int SSZ>
 constexpr size_t smem_bytes() {
-  return ((WARPS * STAGES * 8 + 127) / 128) * 128 + (size_t)WARPS * STAGES * stage_bytes<VT>();
+  return ((WARPS * STAGES * 8 + 127) / 128) * 128 + (size_t)WARPS * STAGES * stage_bytes<VT, SSZ>();
 }
 
+template <int SSZ>
 __device__ __forceinline__ uint32_t seg_nst(size_t seg, size_t seg_slots, size_t nslots_pad) {
   const size_t s0 = seg * seg_slots;
   if (s0 >= nslots_pad) return 0;
   const size_t left = nslots_pad - s0;
-  return (uint32_t)((left < seg_slots ? left : seg_slots) / SS);
+  return (uint32_t)((left < seg_slots ? left : seg_slots) / SSZ);
 }
 
-template <typename VT, int WARPS, int STAGES>
+template <typename VT, int WARPS, int STAGES, int SSZ>
 __global__ void __launch_bounds__(WARPS * 32) stream_tma(size_t nslots, size_t nslots_pad, size_t seg_slots,
                                                          size_t nseg, const VT *__restrict__ val,
                                                          const UIN *__restrict__ col, const UIN *__restrict__ heads,
                                                          const UIN *__restrict__ segh, const FPT *__restrict__ x,
                                                          seg::Out o, int *status) {
-  constexpr uint32_t VB = SS * sizeof(VT), CB = SS * 4, HB = SS / 8, STB = VB + CB + HB;
+  constexpr uint32_t VB = SSZ * sizeof(VT), CB = SSZ * 4, HB = SSZ / 8, STB = VB + CB + HB;
+  constexpr int NB = SSZ / BATCH;  // batches per stage
   extern __shared__ __align__(128) unsigned char smem[];
   const int wib = threadIdx.x >> 5;
   const unsigned lane = threadIdx.x & 31u;
@@ -488,13 +686,13 @@ __global__ void __launch_bounds__(WARPS * 32) stream_tma(size_t nslots, size_t n
   size_t pseg = gw, cseg = gw;
   uint32_t pst = 0, cst = 0;
   auto issue = [&](int s) {
-    const size_t b = pseg * seg_slots + (size_t)pst * SS;
+    const size_t b = pseg * seg_slots + (size_t)pst * SSZ;
     unsigned char *dst = ring + (size_t)s * STB;
     tma::bar_expect_tx(&bars[s], STB);
     tma::bulk_g2s(dst, val + b, VB, &bars[s], pol);
     tma::bulk_g2s(dst + VB, col + b, CB, &bars[s], pol);
     tma::bulk_g2s(dst + VB + CB, heads + b / 32, HB, &bars[s], pol);
-    if (++pst >= seg_nst(pseg, seg_slots, nslots_pad)) {
+    if (++pst >= seg_nst<SSZ>(pseg, seg_slots, nslots_pad)) {
       pseg += GW;
       pst = 0;
     }
@@ -515,12 +713,12 @@ __global__ void __launch_bounds__(WARPS * 32) stream_tma(size_t nslots, size_t n
     const VT *sv = reinterpret_cast<const VT *>(stage);
     const UIN *sc = reinterpret_cast<const UIN *>(stage + VB);
     const UIN *shd = reinterpret_cast<const UIN *>(stage + VB + CB);
-    const size_t b = cseg * seg_slots + (size_t)cst * SS;
+    const size_t b = cseg * seg_slots + (size_t)cst * SSZ;
     if (cst == 0) begin(st, o, cseg, segh[cseg], shd[0]);
-    double p[4][4];
-    Words<4> hw[4];
+    double p[NB][4];
+    Words<4> hw[NB];
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
+    for (int j = 0; j < NB; j++) {
       const int i0 = BATCH * j + 4 * (int)lane;
       const uint4 c = *reinterpret_cast<const uint4 *>(sc + i0);
       const UIN cc[4] = {c.x, c.y, c.z, c.w};
@@ -534,7 +732,7 @@ __global__ void __launch_bounds__(WARPS * 32) stream_tma(size_t nslots, size_t n
       issue(s);
     }
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
+    for (int j = 0; j < NB; j++) {
       const size_t sl = b + BATCH * j + 4 * lane;
       if (sl + 4 > nslots) {
 #pragma unroll
@@ -543,7 +741,7 @@ __global__ void __launch_bounds__(WARPS * 32) stream_tma(size_t nslots, size_t n
       }
       batch<4>(p[j], hw[j], st, o);
     }
-    if (++cst >= seg_nst(cseg, seg_slots, nslots_pad)) {
+    if (++cst >= seg_nst<SSZ>(cseg, seg_slots, nslots_pad)) {
       finish(st, o);
       cseg += GW;
       cst = 0;

@@ -56,6 +56,12 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       : "memory");
 }
 
+// Prefetches `bytes` (a multiple of 16, 16-byte aligned) of global memory
+// into L2 through the bulk-copy engine; no registers or shared memory.
+__device__ __forceinline__ void prefetch_l2(const void *src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(src), "r"(bytes) : "memory");
+}
+
 __device__ __forceinline__ bool bar_try_wait(uint64_t *bar, uint32_t parity) {
   uint32_t ok;
   asm volatile(

@@ -514,3 +514,47 @@ API str_formatData getFormatDataAXT(const UIN ompNT, const UIN bs, const UIN thw
   if (st) die("getFormatDataAXT", st);
   return fd;
 }
+
+/* ------------------------------------------------- batched matrices -- */
+/* Block-diagonal CSR of `count` square matrices: matrix m's rows and columns
+ * start at off[m] (off has count+1 entries).  Arrays are malloc'd (free with
+ * ispmv_csr_free); rl and the statistics are filled. */
+API int ispmv_csr_blockdiag(UIN count, const str_matCSR *mats, str_matCSR *out, UIN *off) {
+  if (!mats || !out || !off || count == 0) return ISPMV_ERR_ARG;
+  uint64_t n = 0, nnz = 0;
+  for (UIN m = 0; m < count; m++) {
+    if (!mats[m].row || mats[m].nrows == 0) return ISPMV_ERR_ARG;
+    off[m] = (UIN)n;
+    n += mats[m].nrows;
+    nnz += mats[m].row[mats[m].nrows];
+    if (n >= 0xFFFFFFFFull || nnz > 0xFFFFFFFFull) return ISPMV_ERR_OVERFLOW;
+  }
+  off[count] = (UIN)n;
+  memset(out, 0, sizeof *out);
+  out->nrows = (UIN)n;
+  out->nnz = (UIN)nnz;
+  out->row = (UIN *)malloc(((size_t)n + 1) * sizeof(UIN));
+  out->rl = (UIN *)calloc((size_t)n + 1, sizeof(UIN));
+  out->col = (UIN *)malloc((size_t)(nnz ? nnz : 1) * sizeof(UIN));
+  out->val = (FPT *)malloc((size_t)(nnz ? nnz : 1) * sizeof(FPT));
+  if (!out->row || !out->rl || !out->col || !out->val) {
+    free(out->row); free(out->rl); free(out->col); free(out->val);
+    memset(out, 0, sizeof *out);
+    return ISPMV_ERR_OOM;
+  }
+  uint64_t j = 0;
+  out->row[0] = 0;
+  for (UIN m = 0; m < count; m++) {
+    const str_matCSR *a = &mats[m];
+    const UIN base = off[m], an = a->nrows, annz = a->row[an];
+    for (UIN r = 0; r < an; r++) out->row[base + r + 1] = (UIN)j + a->row[r + 1];
+    for (UIN q = 0; q < annz; q++) {
+      if (a->col[q] >= an) { free(out->row); free(out->rl); free(out->col); free(out->val);
+        memset(out, 0, sizeof *out); return ISPMV_ERR_ARG; }
+      out->col[j + q] = a->col[q] + base;
+      out->val[j + q] = a->val[q];
+    }
+    j += annz;
+  }
+  return ispmv_csr_stats(out);
+}

@@ -92,11 +92,12 @@ KERNELS = {"auto": abi.KERNEL_AUTO, "ldg": abi.KERNEL_LDG, "tma": abi.KERNEL_TMA
 
 
 def plan_opts(val="f64", col="u32", kernel="auto", units_per_warp=0, ctas_per_sm=0, lo_tol=0.0,
-              variant=0) -> abi.PlanOpts:
+              variant=0, rhs_block=0) -> abi.PlanOpts:
     o = abi.PlanOpts()
     load().ispmv_plan_opts_default(C.byref(o))
     o.val_kind, o.col_kind, o.kernel = VAL_KINDS[val], COL_KINDS[col], KERNELS[kernel]
     o.units_per_warp, o.ctas_per_sm, o.lo_tol, o.variant = units_per_warp, ctas_per_sm, lo_tol, variant
+    o.rhs_block = rhs_block
     return o
 
 
@@ -106,10 +107,10 @@ class Plan:
     False = int_k1 then orderArrayK1)."""
 
     def __init__(self, csr: CSR, fmt: AXC | K1 | AXT | None = None, *, reorder: bool = True, val="f64", col="u32",
-                 kernel="auto", units_per_warp=0, ctas_per_sm=0, lo_tol=0.0, variant=0,
+                 kernel="auto", units_per_warp=0, ctas_per_sm=0, lo_tol=0.0, variant=0, rhs_block=0,
                  axi: np.ndarray | None = None):
         lib = load()
-        o = plan_opts(val, col, kernel, units_per_warp, ctas_per_sm, lo_tol, variant)
+        o = plan_opts(val, col, kernel, units_per_warp, ctas_per_sm, lo_tol, variant, rhs_block)
         h = C.c_void_p()
         if fmt is None:
             check(lib.ispmv_plan_csr(C.byref(csr.c), C.byref(o), C.byref(h)), "ispmv_plan_csr")
@@ -151,12 +152,34 @@ class Plan:
         """ISPMV_ERR_TIMEOUT if a bounded device wait gave up, else 0 (syncs)."""
         return int(load().ispmv_plan_status(self._h))
 
+    def time_kernels(self, pairs: int) -> None:
+        """Record a CUDA event pair around the main kernel of each spmv
+        (a ring of `pairs`; 0 turns it off)."""
+        check(load().ispmv_plan_time_kernels(self._h, int(pairs)), "ispmv_plan_time_kernels")
+
+    def kernel_ms(self) -> tuple[float, int]:
+        """(summed main-kernel milliseconds, pairs) since the last call; the
+        stream must be synchronised first."""
+        ms, n = C.c_double(), C.c_int()
+        check(load().ispmv_plan_kernel_ms(self._h, C.byref(ms), C.byref(n)), "ispmv_plan_kernel_ms")
+        return ms.value, n.value
+
+    def kernel_name(self) -> str:
+        """The main kernel of the latest product (e.g. "stream_ldg<4,0,5>")."""
+        return load().ispmv_plan_kernel_name(self._h).decode()
+
     def spmv(self, x: torch.Tensor, y: torch.Tensor | None = None, beta: int = 0, stream=None) -> torch.Tensor:
         if x.dtype != torch.float64 or x.numel() != self.n:
             raise ValueError("x must be a float64 CUDA tensor of n entries")
         if y is None:
             y = torch.empty(self.n, dtype=torch.float64, device=x.device)
         check(load().ispmv_plan_spmv(self._h, _ptr(x), _ptr(y), int(beta), _stream(stream)), "ispmv_plan_spmv")
+        return y
+
+    def spmv_graph(self, x: torch.Tensor, y: torch.Tensor, beta: int = 0, stream=None) -> torch.Tensor:
+        """spmv as one CUDA-graph launch (captured on first use for these x, y)."""
+        check(load().ispmv_plan_spmv_graph(self._h, _ptr(x), _ptr(y), int(beta), _stream(stream)),
+              "ispmv_plan_spmv_graph")
         return y
 
     def spmm(self, X: torch.Tensor, Y: torch.Tensor | None = None, stream=None) -> torch.Tensor:

@@ -143,3 +143,16 @@ def test_errors_and_initvec():
     res = np.array([1.0, 2.5, -3.0])  # sign errors are invisible to the reference metric
     a, r, p = F.getErrors(ref, res)
     assert (a, p) == (0.5, 1) and r == 0.5 / 3.0
+
+
+def test_blockdiag_host():
+    from int_spmv_b200 import batch as B
+    mats = [M.random_csr(n, s, rl_max=12, empty_frac=0.1) for n, s in ((50, 1), (7, 2), (300, 3))]
+    big, off = B.blockdiag(mats)
+    assert list(off) == [0, 50, 57, 357]
+    assert big.n == 357 and big.nnz == sum(len(c) for _, c, _ in mats)
+    for m, (row, col, val) in enumerate(mats):
+        a = int(off[m])
+        r0 = int(big.row[a])
+        assert np.array_equal(big.col[r0:r0 + len(col)], col.astype(np.int64) + a)
+        assert np.array_equal(big.val[r0:r0 + len(val)], val)

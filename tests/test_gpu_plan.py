@@ -84,14 +84,40 @@ def test_segment_boundaries(env, fmt, kernel):
 
 
 @pytest.mark.parametrize("fmt", ["COM128", "NOC1", "AXC", "CSR"])
-@pytest.mark.parametrize("variant", list(range(12)))
+@pytest.mark.parametrize("variant", list(range(16)) + [17, 18, 19, 20])
 def test_stream_variants(env, fmt, variant):
     from int_spmv_b200 import matrices as M
     row, col, val = M.random_csr(7001, 12, rl_max=90, empty_frac=0.1)
     x = M.uniform_x(7001, 12)
-    for ctas in (1, 2, 3):
+    check_plan(env, row, col, val, x, fmt, kernel="ldg", variant=variant)
+    if variant < 4:
+        for ctas in (0, 1):
+            p, _ = check_plan(env, row, col, val, x, fmt, kernel="tma", variant=variant, ctas_per_sm=ctas)
+            assert p.status() == 0
+
+
+@pytest.mark.parametrize("case", ["poisson", "stencil", "banded_empty"])
+@pytest.mark.parametrize("variant", [8, 9, 10, 11, 17, 18, 19, 20])
+def test_xband_variants(env, case, variant):
+    """Shared-memory x bands: matrices whose columns sit in diagonal bands,
+    so the bands are chosen and most gathers read shared memory."""
+    from int_spmv_b200 import matrices as M
+    if case == "poisson":
+        row, col, val = M.poisson2d(180)
+    elif case == "stencil":
+        row, col, val = M.stencil27(24)
+    else:
+        row, col, val = M.fem_banded(20011, np.random.default_rng(5), 3, 30)
+        rl = np.diff(row).astype(np.int64)
+        rows = np.repeat(np.arange(len(rl)), rl)
+        keep = rows % 17 != 0  # every 17th row empty
+        rl = np.bincount(rows[keep], minlength=len(rl))
+        row = np.concatenate([[0], np.cumsum(rl)]).astype(row.dtype)
+        col, val = col[keep], val[keep]
+    n = len(row) - 1
+    x = M.uniform_x(n, 3)
+    for fmt in ("COM128", "NOC1"):
         check_plan(env, row, col, val, x, fmt, kernel="ldg", variant=variant)
-        check_plan(env, row, col, val, x, fmt, kernel="tma", ctas_per_sm=ctas)
 
 
 @pytest.mark.parametrize("fmt,kernel", [("NOC1", "ldg"), ("NOC4", "tma"), ("COM128", "ldg"), ("COM128", "tma"),
@@ -188,3 +214,32 @@ def test_precision_forms_rejected_elsewhere(env):
         make_plan(F, D, csr, g["x"], "NOC4", val="f32lo", kernel="ldg")
     with pytest.raises(IntSpmvError):
         make_plan(F, D, csr, g["x"], "CSR", col="d16", kernel="rows")
+
+
+@pytest.mark.parametrize("fmt,kernel", [("COM128", "ldg"), ("NOC4", "tma"), ("K1", "auto"), ("CSR", "rows")])
+def test_kernel_timing_events(env, fmt, kernel):
+    """Event pairs around the main kernel: one pair per spmv (a ring of the
+    latest), none for graph launches, and the product unchanged."""
+    torch, D, F, orc = env
+    from int_spmv_b200 import matrices as M
+    row, col, val = M.random_csr(50000, 21, rl_max=40)
+    x = M.uniform_x(50000, 21)
+    csr = F.CSR(row, col, val)
+    p = make_plan(F, D, csr, x, fmt, kernel=kernel)
+    xt = torch.from_numpy(x).cuda()
+    y = torch.empty_like(xt)
+    p.time_kernels(4)
+    for _ in range(6):
+        p.spmv(xt, y)
+    torch.cuda.synchronize()
+    ms, n = p.kernel_ms()
+    assert n == 4 and ms > 0
+    assert p.kernel_name()
+    p.spmv_graph(xt, y)
+    torch.cuda.synchronize()
+    assert p.kernel_ms() == (0.0, 0)
+    p.time_kernels(0)
+    p.spmv(xt, y)
+    torch.cuda.synchronize()
+    assert p.kernel_ms() == (0.0, 0)
+    assert_parity(y.cpu().numpy(), orc.cf_csr(row, col, val, x), orc.abs_csr(row, col, val, x), TOL_F64)
