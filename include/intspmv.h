@@ -262,6 +262,9 @@ typedef struct ispmv_plan_s *ispmv_plan;
 #define ISPMV_KERNEL_LDG 1   /* slot-stream kernel, plain loads, register prefetch */
 #define ISPMV_KERNEL_TMA 2   /* slot-stream kernel, 1D bulk copies (cp.async.bulk) into shared memory */
 #define ISPMV_KERNEL_ROWS 3  /* row-parallel kernel (CSR: lanes per row; AXC: 8 lanes per row; K1) */
+#define ISPMV_KERNEL_WIDE 4  /* slot-stream kernel over a lane-interleaved copy of the stream: 16 (or 8)
+                                slots per lane, diagonal x bands in shared memory (FP64/FP32 values,
+                                u32 columns; SpMV only) */
 #define ISPMV_VARIANT_QUEUE 16 /* slot-stream kernel as a work queue drained by persistent warps */
 
 typedef struct {

@@ -137,5 +137,5 @@ PROTOTYPES: dict[str, tuple] = {
 OK, ERR_ARG, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_OVERFLOW = range(7)
 VAL_F64, VAL_F32, VAL_F32_LO16 = 0, 1, 2
 COL_U32, COL_D16 = 0, 1
-KERNEL_AUTO, KERNEL_LDG, KERNEL_TMA, KERNEL_ROWS = 0, 1, 2, 3
+KERNEL_AUTO, KERNEL_LDG, KERNEL_TMA, KERNEL_ROWS, KERNEL_WIDE = 0, 1, 2, 3, 4
 VARIANT_QUEUE = 16

@@ -9,7 +9,8 @@
 //           col[S] zero-padded to a multiple of 512 slots, a row-start bitmap
 //           (1 bit per slot), per-segment start counts, and the compressed ->
 //           real row map when some rows are empty.  Kernels: sss::stream_ldg,
-//           sss::stream_tma.
+//           sss::stream_tma; wide::stream_wide reads val/col from a
+//           lane-interleaved copy (wide::il_pos) instead of slot order.
 //   units   AXT NOC tileH>1 (tile columns): val/col in tile order plus the
 //           reference's per-column row array (sec) cut to the used columns.
 //           Kernels: pk::noc_hn, tk::nocn_tma.
@@ -25,6 +26,7 @@
 #include "plan_tma.cuh"
 #include "spmm.cuh"
 #include "sss.cuh"
+#include "wide.cuh"
 
 using namespace ispmv;
 
@@ -167,7 +169,7 @@ int begin(const ispmv_plan_opts *o, ispmv_plan_s **out) {
   if (o) p->opts = *o;
   else ispmv_plan_opts_default(&p->opts);
   if (p->opts.val_kind < ISPMV_VAL_F64 || p->opts.val_kind > ISPMV_VAL_F32_LO16 || p->opts.col_kind < ISPMV_COL_U32 ||
-      p->opts.col_kind > ISPMV_COL_D16 || p->opts.kernel < 0 || p->opts.kernel > ISPMV_KERNEL_ROWS) {
+      p->opts.col_kind > ISPMV_COL_D16 || p->opts.kernel < 0 || p->opts.kernel > ISPMV_KERNEL_WIDE) {
     delete p;
     return ISPMV_ERR_UNSUPPORTED;
   }
@@ -223,6 +225,32 @@ bool xw_variant(int v, XwCfg *c) {
   }
 }
 
+// stream_wide variants: slots per lane; x bands in shared memory (plain
+// loads only) and shared doubles for them; segment slots; CTAs per SM the
+// registers are sized for (plain loads); rows through a per-warp buffer
+// (coalesced y stores) or written by the lane that ends them; and for the
+// staged form (tma) the stages per warp and warps per CTA.
+struct WideCfg { int spl; bool win; UIN cap; size_t seg; int minb; bool buf; bool tma; int stages; int warps; };
+constexpr int WIDE_WARPS = 8;
+WideCfg wide_variant(int v) {
+  switch (v) {
+    case 1: return {16, false, 0, 4096, 3, true, false, 0, 8};
+    case 2: return {16, true, 6144, 4096, 2, false, false, 0, 8};
+    case 3: return {16, true, 6144, 4096, 2, true, false, 0, 8};
+    case 4: return {8, false, 0, 2048, 4, false, false, 0, 8};
+    case 5: return {8, false, 0, 2048, 4, true, false, 0, 8};
+    case 6: return {16, true, 4096, 2048, 2, false, false, 0, 8};
+    case 7: return {8, true, 4096, 4096, 4, false, false, 0, 8};
+    case 8: return {16, false, 0, 8192, 3, false, false, 0, 8};
+    case 9: return {16, false, 0, 2048, 3, false, false, 0, 8};
+    case 10: return {8, false, 0, 4096, 0, false, true, 3, 8};
+    case 11: return {16, false, 0, 4096, 0, false, true, 2, 4};
+    case 12: return {16, false, 0, 4096, 0, false, true, 3, 4};
+    case 13: return {8, false, 0, 4096, 0, false, true, 4, 4};
+    default: return {16, false, 0, 4096, 3, false, false, 0, 8};
+  }
+}
+
 // Picks up to 3 diagonal bands (offset, half-width) of col - row from a
 // deterministic sample of the nonzeros: the densest interval that fits the
 // budget, then the densest of what is left, while a band holds >= 5% of the
@@ -272,8 +300,6 @@ int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v,
   p->slots_pad = std::max(SS, (p->slots + SS - 1) / SS * SS);
   v.resize(p->slots_pad, 0.0);
   c.resize(p->slots_pad, 0);
-  TRY(upload_values(p, v));
-  if (p->opts.col_kind == ISPMV_COL_U32) TRY(dev_upload(p, c.data(), c.size(), &p->col));
   std::vector<UIN> heads(p->slots_pad / 32, 0), rowmap;
   bool any_empty = false;
   for (UIN r = 0; r < p->n; r++) {
@@ -286,8 +312,17 @@ int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v,
     rowmap.push_back(r);
   }
   XwCfg xc;
-  const bool xwv = p->opts.kernel == ISPMV_KERNEL_LDG && !narrow_kinds(p) && xw_variant(p->opts.variant, &xc);
+  bool xwv = p->opts.kernel == ISPMV_KERNEL_LDG && !narrow_kinds(p) && xw_variant(p->opts.variant, &xc);
+  const bool wide = p->opts.kernel == ISPMV_KERNEL_WIDE;
+  if (wide) {
+    if (narrow_kinds(p)) return fail(ISPMV_ERR_UNSUPPORTED, "stream_wide: FP64/FP32 values with u32 columns only");
+    const WideCfg wc = wide_variant(p->opts.variant);
+    xc = {wc.warps, wc.cap, wc.seg};
+    xwv = wc.win;
+  }
   p->seg_slots = xwv && p->opts.units_per_warp <= 0 ? xc.seg : seg_slots_of(p, 1);
+  if (wide && p->opts.units_per_warp <= 0) p->seg_slots = xc.seg;
+  if (wide && p->seg_slots % SS) p->seg_slots = (p->seg_slots + SS - 1) / SS * SS;
   p->nseg = (p->slots_pad + p->seg_slots - 1) / p->seg_slots;
   std::vector<UIN> segh(std::max<size_t>(1, p->nseg), 0);
   UIN acc = 0;
@@ -295,6 +330,22 @@ int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v,
     const size_t wend = std::min(heads.size(), (sg * p->seg_slots) >> 5);
     for (; w < wend; w++) acc += __builtin_popcount(heads[w]);
     segh[sg] = acc;
+  }
+  if (wide) {
+    // the lane-interleaved copy: batches of 32*spl slots, one 16-byte vector per lane and step
+    const unsigned spl = (unsigned)wide_variant(p->opts.variant).spl;
+    std::vector<double> vi(p->slots_pad);
+    std::vector<UIN> ci(p->slots_pad);
+    const unsigned vv = p->opts.val_kind == ISPMV_VAL_F64 ? 2u : 4u;
+    for (size_t q = 0; q < p->slots_pad; q++) {
+      vi[wide::il_pos(q, spl, vv)] = v[q];
+      ci[wide::il_pos(q, spl, 4u)] = c[q];
+    }
+    TRY(upload_values(p, vi));
+    TRY(dev_upload(p, ci.data(), ci.size(), &p->col));
+  } else {
+    TRY(upload_values(p, v));
+    if (p->opts.col_kind == ISPMV_COL_U32) TRY(dev_upload(p, c.data(), c.size(), &p->col));
   }
   if (p->opts.col_kind == ISPMV_COL_D16) {
     // per 128-slot batch: base = the smallest column among nonzero values;
@@ -606,8 +657,72 @@ int launch_staged_w(K kernel, size_t smem, size_t nseg, int ctas_per_sm, cudaStr
   return check_launch(what);
 }
 
+template <typename VT, int SPL, int NW, int MINB, bool BUF>
+int launch_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, const char *name) {
+  auto *k = wide::stream_wide<VT, SPL, NW, WIDE_WARPS, MINB, BUF>;
+  const size_t smem =
+      ((NW ? (size_t)p->xw.cap : 0) + (BUF ? (size_t)WIDE_WARPS * 32 * SPL : 0)) * sizeof(double);
+  if (smem) ISPMV_TRY(cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const unsigned g = (unsigned)((p->nseg + WIDE_WARPS - 1) / WIDE_WARPS);
+  k<<<g, WIDE_WARPS * 32, smem, s>>>(p->slots, p->slots_pad, p->seg_slots, p->nseg, static_cast<const VT *>(p->val),
+                                      p->col, p->heads, p->segh, p->xw, x, o);
+  return check_launch(name);
+}
+
+// The staged form: persistent, as many CTAs as fit on the SMs (at most one
+// warp per segment).
+template <typename VT, int SPL, int STAGES, int W>
+int launch_wide_tma(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, const char *name) {
+  auto *k = wide::stream_wide_tma<VT, SPL, STAGES, W, false>;
+  const size_t smem = wide::tma_smem_bytes<VT, SPL, STAGES, W, false>();
+  ISPMV_TRY(cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  ISPMV_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, W * 32, smem));
+  if (p->opts.ctas_per_sm > 0) per_sm = std::min(per_sm, p->opts.ctas_per_sm);
+  const size_t want = (p->nseg + W - 1) / W;
+  const unsigned g = (unsigned)std::max<size_t>(1, std::min(want, (size_t)sm_count() * (size_t)std::max(1, per_sm)));
+  k<<<g, W * 32, smem, s>>>(p->slots, p->slots_pad, p->seg_slots, p->nseg, static_cast<const VT *>(p->val), p->col,
+                            p->heads, p->segh, x, o, p->status);
+  return check_launch(name);
+}
+
+// stream_wide<slots per lane, x bands, CTAs per SM, row buffer> for 0..3 bands.
+#define ISPMV_WIDE_NW(SPL, MINB, BUF)                                                                        \
+  switch (nw) {                                                                                              \
+    case 0: return launch_wide<VT, SPL, 0, MINB, BUF>(p, x, o, s, "stream_wide<" #SPL ",w0,b" #MINB ",buf" #BUF ">"); \
+    case 1: return launch_wide<VT, SPL, 1, MINB, BUF>(p, x, o, s, "stream_wide<" #SPL ",w1,b" #MINB ",buf" #BUF ">"); \
+    case 2: return launch_wide<VT, SPL, 2, MINB, BUF>(p, x, o, s, "stream_wide<" #SPL ",w2,b" #MINB ",buf" #BUF ">"); \
+    default: return launch_wide<VT, SPL, 3, MINB, BUF>(p, x, o, s, "stream_wide<" #SPL ",w3,b" #MINB ",buf" #BUF ">"); \
+  }
+
+template <typename VT>
+int run_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
+  const WideCfg wc = wide_variant(p->opts.variant);
+  if (wc.tma) {
+    switch (p->opts.variant) {
+      case 10: return launch_wide_tma<VT, 8, 3, 8>(p, x, o, s, "stream_wide_tma<8,s3,w8>");
+      case 11: return launch_wide_tma<VT, 16, 2, 4>(p, x, o, s, "stream_wide_tma<16,s2,w4>");
+      case 12: return launch_wide_tma<VT, 16, 3, 4>(p, x, o, s, "stream_wide_tma<16,s3,w4>");
+      default: return launch_wide_tma<VT, 8, 4, 4>(p, x, o, s, "stream_wide_tma<8,s4,w4>");
+    }
+  }
+  const int nw = wc.win ? std::min(std::max(p->xw.nwin, 0), 3) : 0;
+  if (wc.spl == 8) {
+    if (wc.buf) { ISPMV_WIDE_NW(8, 4, 1) }
+    ISPMV_WIDE_NW(8, 4, 0)
+  }
+  if (wc.win) {
+    if (wc.buf) { ISPMV_WIDE_NW(16, 2, 1) }
+    ISPMV_WIDE_NW(16, 2, 0)
+  }
+  if (wc.buf) return launch_wide<VT, 16, 0, 3, 1>(p, x, o, s, "stream_wide<16,w0,b3,buf1>");
+  return launch_wide<VT, 16, 0, 3, 0>(p, x, o, s, "stream_wide<16,w0,b3,buf0>");
+}
+#undef ISPMV_WIDE_NW
+
 template <typename VT>
 int run_stream(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
+  if (p->opts.kernel == ISPMV_KERNEL_WIDE) return run_wide<VT>(p, x, o, s);
   const VT *val = static_cast<const VT *>(p->val);
   size_t nslots = p->slots, spad = p->slots_pad, sslots = p->seg_slots, nseg = p->nseg;
   const UIN *col = p->col, *heads = p->heads, *segh = p->segh;
@@ -966,8 +1081,8 @@ int spmm_run(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
 // (AXT COM, AXT tileH=1, AXC and CSR built with the stream kernels).
 ISPMV_API int ispmv_plan_spmm(ispmv_plan p, UIN k, const FPT *X, FPT *Y, void *stream) {
   if (!p || !X || !Y || k == 0) return ISPMV_ERR_ARG;
-  if (p->path != P_STREAM || narrow_kinds(p))
-    return fail(ISPMV_ERR_UNSUPPORTED, "ispmv_plan_spmm: needs a slot-stream plan with u32 columns");
+  if (p->path != P_STREAM || narrow_kinds(p) || p->opts.kernel == ISPMV_KERNEL_WIDE)
+    return fail(ISPMV_ERR_UNSUPPORTED, "ispmv_plan_spmm: needs a slot-stream plan with u32 columns in slot order");
   cudaStream_t s = as_stream(stream);
   if (!p->slots) {  // every row empty
     ISPMV_TRY(cudaMemsetAsync(Y, 0, (size_t)p->n * k * sizeof(FPT), s));

@@ -1,0 +1,463 @@
+// wide.cuh - the slot-stream SpMV over a lane-interleaved copy of the
+// stream, 8 or 16 slots per lane, with the x bands a CTA's rows need staged
+// in shared memory.
+//
+// Why: on B200 the 4-slot-per-lane kernel (stream_ldg) is bound by the L1
+// data path, not by HBM.  A warp-wide gather of 32 unrelated columns costs
+// one L1 wavefront per distinct 128-byte line (about one per nonzero), and
+// its segmented warp scan runs once per 128 slots (about 1.7 instructions
+// per nonzero).  This kernel:
+//   - runs one warp scan per 32*SPL slots (SPL = 16: 512), so the
+//     warp-level reduction costs about 0.15 instructions per nonzero;
+//   - reads values and columns with coalesced 16-byte loads from a copy of
+//     the stream stored lane-interleaved: per batch of 32*SPL slots, lane l
+//     owns the SPL consecutive slots b + SPL*l + k, and element (l, k) sits at
+//     b + (k / V)*32*V + l*V + k % V with V = 16 / sizeof(element), so every
+//     vector load of the warp is 512 contiguous bytes;
+//   - gathers a column that falls in one of the plan's diagonal bands from
+//     shared memory (a few bank wavefronts per warp instead of up to 32 L1
+//     wavefronts), and any other column from x through L1/L2.  Which path
+//     serves a column does not change the result.
+// The row reduction is the slot stream's: rows are contiguous runs of
+// slots, row starts are bits of `heads` (slot order), a warp owns a segment
+// of slots and leaves two (row, partial) records per segment for
+// seg::fixup.  The rows a batch completes pass through a per-warp buffer in
+// shared memory and reach y as coalesced stores.  Every row is written
+// exactly once, without atomics, and the summation order is fixed, so
+// results are bitwise repeatable.
+//
+// stream_wide_tma is the same reduction fed by 1D bulk copies
+// (cp.async.bulk, no multicast) into a per-warp ring of stages in shared
+// memory: one lane keeps the next stages of its warp's segments in flight,
+// so the value/column stream leaves both the warp's critical path and the
+// L1 load pipe.
+#pragma once
+#include "sss.cuh"
+
+namespace ispmv {
+namespace wide {
+
+// Position of slot s in the lane-interleaved copy (32*spl-slot batches,
+// v elements per vector load).
+__host__ __device__ inline size_t il_pos(size_t s, unsigned spl, unsigned v) {
+  const size_t bt = 32u * spl;
+  const size_t b = s / bt * bt;
+  const unsigned r = (unsigned)(s - b), l = r / spl, k = r % spl;
+  return b + (size_t)(k / v) * 32u * v + (size_t)l * v + k % v;
+}
+
+template <typename VT, int SPL>
+struct Vals;
+template <int SPL>
+struct Vals<double, SPL> {
+  double2 q[SPL / 2];
+  __device__ __forceinline__ void get(const double *v, size_t b, unsigned lane) {
+#pragma unroll
+    for (int i = 0; i < SPL / 2; i++) q[i] = ld_stream(reinterpret_cast<const double2 *>(v + b + 64 * i + 2 * lane));
+  }
+  __device__ __forceinline__ double operator[](int k) const { return (k & 1) ? q[k >> 1].y : q[k >> 1].x; }
+};
+template <int SPL>
+struct Vals<float, SPL> {
+  float4 q[SPL / 4];
+  __device__ __forceinline__ void get(const float *v, size_t b, unsigned lane) {
+#pragma unroll
+    for (int i = 0; i < SPL / 4; i++) q[i] = ld_stream(reinterpret_cast<const float4 *>(v + b + 128 * i + 4 * lane));
+  }
+  __device__ __forceinline__ float operator[](int k) const {
+    const float4 &t = q[k >> 2];
+    return (k & 3) == 0 ? t.x : (k & 3) == 1 ? t.y : (k & 3) == 2 ? t.z : t.w;
+  }
+};
+
+template <int SPL>
+struct Cols {
+  uint4 q[SPL / 4];
+  __device__ __forceinline__ void get(const UIN *c, size_t b, unsigned lane) {
+#pragma unroll
+    for (int i = 0; i < SPL / 4; i++) q[i] = ld_stream(reinterpret_cast<const uint4 *>(c + b + 128 * i + 4 * lane));
+  }
+  __device__ __forceinline__ UIN operator[](int k) const {
+    const uint4 &t = q[k >> 2];
+    return (k & 3) == 0 ? t.x : (k & 3) == 1 ? t.y : (k & 3) == 2 ? t.z : t.w;
+  }
+};
+
+// The bands of x a CTA stages: band k holds columns [lo[k], lo[k] + len[k])
+// at shared-memory offset lo[k] + delta[k] (u32 arithmetic, modulo 2^32).
+template <int NW>
+struct Bands {
+  UIN lo[NW > 0 ? NW : 1], len[NW > 0 ? NW : 1], delta[NW > 0 ? NW : 1];
+};
+
+// x[c]: from a shared-memory band when c falls in one, else through L1/L2.
+// Two predicated loads into one register: the shared-memory load runs on
+// the lanes whose column is in a band, the global load on the others.
+template <int NW>
+__device__ __forceinline__ double gather(const Bands<NW> &w, uint32_t sx_addr, const FPT *__restrict__ x, UIN c) {
+  if constexpr (NW == 0) {
+    return __ldg(x + c);
+  } else {
+    uint32_t in = 0, off = 0;
+#pragma unroll
+    for (int k = 0; k < NW; k++) {
+      if (c - w.lo[k] < w.len[k]) {  // band starts lie in [0, n]: the unsigned difference is exact
+        in = 1;
+        off = c + w.delta[k];
+      }
+    }
+    double v;
+    asm volatile(
+        "{\n"
+        ".reg .pred p;\n"
+        "setp.ne.u32 p, %3, 0;\n"
+        "@p ld.shared.f64 %0, [%1];\n"
+        "@!p ld.global.nc.f64 %0, [%2];\n"
+        "}\n"
+        : "=d"(v)
+        : "r"(sx_addr + 8u * off), "l"(x + c), "r"(in));
+    return v;
+  }
+}
+
+// One batch of 32*SPL slots: lane l holds the values v[k] and gathered x
+// values xv[k] of slots b + SPL*l + k, and `bits`, its SPL row-start bits
+// (bit k = slot k).  Each lane sums its slots in slot order into `pre`
+// (slots before its first row start), the rows that start and end in it,
+// and `acc` (the run from its last row start); one segmented warp scan then
+// joins the pieces of rows that cross lanes.  When no lane of the warp
+// holds two row starts (rows longer than SPL slots), the lane pass is two
+// predicated multiply-adds per slot; otherwise the rows that end inside a
+// lane are written as they end.  Both paths add the same products in the
+// same order, so the result does not depend on the path.
+//
+// BUF: the rows the batch completes are entries e = 0 .. tot-1 of `rbuf`
+// (the warp's 32*SPL doubles), e = row - (st.rbase - 1); entry 0 is the row
+// open at the batch start, entry i the row of the batch's i-th start.  The
+// warp then stores the entries to y with coalesced stores.  !BUF: every row
+// goes to y (or to the segment's head record) from the lane that ends it.
+template <typename VT, int SPL, bool BUF>
+__device__ __forceinline__ void batch(const VT (&v)[SPL], const double (&xv)[SPL], unsigned bits, sss::Run &st,
+                                      const seg::Out &o, double *rbuf) {
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned cnt = __popc(bits);
+  unsigned incl = cnt;  // row starts up to and including my slots
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const unsigned t = __shfl_up_sync(FULL, incl, d);
+    if ((int)lane >= d) incl += t;
+  }
+  const unsigned tot = __shfl_sync(FULL, incl, 31);
+  const unsigned ex = incl - cnt;   // entry of the row open at my first slot
+  const UIN rb = st.rbase + ex;     // row of my first start
+  const int first = cnt ? __ffs(bits) - 1 : SPL;
+  double pre = 0.0, acc = 0.0;
+  if (__all_sync(FULL, cnt <= 1u)) {
+#pragma unroll
+    for (int k = 0; k < SPL; k++) {
+      if (k < first) pre = pk::fmac<VT>(v[k], xv[k], pre);
+      else acc = pk::fmac<VT>(v[k], xv[k], acc);
+    }
+  } else {
+    UIN r = rb;        // row of the run being summed, once past my first start
+    unsigned e = ex;   // its entry in rbuf, minus one before my first start
+#pragma unroll
+    for (int k = 0; k < SPL; k++) {
+      if ((bits >> k) & 1u) {
+        if (k > first) {  // a row that starts and ends in this lane
+          if constexpr (BUF) {
+            rbuf[e] = acc;
+          } else {
+            seg::write_row(o, r, acc);  // never the segment's open row: it started in this segment
+            r++;
+          }
+        } else {
+          pre = acc;
+        }
+        e++;
+        acc = 0.0;
+      }
+      acc = pk::fmac<VT>(v[k], xv[k], acc);
+    }
+    if (!cnt) {
+      pre = acc;
+      acc = 0.0;
+    }
+  }
+  if (lane == 0 && st.carry) pre += st.csum;
+  // lanes' leading and trailing pieces: one segmented warp scan whose
+  // windows stop at the lane holding the row's start
+  const bool f = cnt != 0;
+  const unsigned F = __ballot_sync(FULL, f) & sss::lanemask_le();
+  const int start = F ? 31 - __clz(F) : 0;
+  const int reach = (int)lane - start;
+  double I = f ? acc : pre;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const double u = __shfl_up_sync(FULL, I, d);
+    if (reach >= d) I += u;
+  }
+  double E = __shfl_up_sync(FULL, I, 1);
+  if (lane == 0) E = 0.0;
+  if constexpr (BUF) {
+    if (f) rbuf[ex] = E + pre;  // the row open at my lane's start ends at my first start
+    // entry 0 exists unless this is the segment's first batch and the
+    // segment starts at a row start
+    const bool valid0 = st.carry || st.row_a != NO_ROW;
+    st.csum = __shfl_sync(FULL, I, 31);
+    st.carry = true;
+    __syncwarp();
+    for (unsigned j = lane; j < tot; j += 32) {
+      const UIN row = st.rbase - 1u + j;
+      const double val = rbuf[j];
+      if (j == 0 && !valid0) continue;
+      if (row == st.row_a) {  // the row open at the segment's first slot: its head record
+        o.rec_row[2 * (size_t)st.seg] = row;
+        o.rec_sum[2 * (size_t)st.seg] = val;
+      } else {
+        seg::write_row(o, row, val);
+      }
+    }
+    __syncwarp();
+  } else {
+    // the run open at my lane's start ends at my first row start
+    if (f && (lane > 0 || !(bits & 1u) || st.carry)) sss::emit(o, st, rb - 1u, E + pre);
+    st.csum = __shfl_sync(FULL, I, 31);
+    st.carry = true;
+  }
+  st.rbase += tot;
+}
+
+// Plain-load form.  MINB CTAs of WARPS*32 threads per SM bound the
+// registers.  NW = number of shared-memory x bands (0: every gather through
+// L1/L2).  Dynamic shared memory: xw.cap doubles of bands (NW > 0), then
+// (BUF) WARPS row buffers of 32*SPL doubles.
+template <typename VT, int SPL, int NW, int WARPS, int MINB, bool BUF>
+__global__ void __launch_bounds__(WARPS * 32, MINB)
+    stream_wide(size_t nslots, size_t nslots_pad, size_t seg_slots, size_t nseg, const VT *__restrict__ val,
+                const UIN *__restrict__ col, const UIN *__restrict__ heads, const UIN *__restrict__ segh,
+                sss::XWin xw, const FPT *__restrict__ x, seg::Out o) {
+  constexpr int BT = 32 * SPL;
+  constexpr unsigned MASK = SPL == 32 ? 0xffffffffu : (1u << SPL) - 1u;
+  extern __shared__ __align__(16) double sx[];
+  __shared__ sss::WinState sw;
+  const unsigned lane = threadIdx.x & 31u;
+  const size_t seg0 = (size_t)blockIdx.x * WARPS;
+  const size_t segid = seg0 + (threadIdx.x >> 5);
+  double *rbuf = sx + (NW > 0 ? xw.cap : 0) + (size_t)(threadIdx.x >> 5) * BT;
+  Bands<NW> w{};
+  if constexpr (NW > 0) {
+    // the CTA's row range, from the start counts of its first and
+    // one-past-last segments, and the bands of x it reads
+    if (threadIdx.x == 0) {
+      const size_t segl = min(seg0 + WARPS, nseg);
+      UIN c0 = segh[seg0];
+      c0 = c0 > 0 ? c0 - 1 : 0;  // the run open at the first slot
+      UIN c1 = segl < nseg ? segh[segl] : xw.nrows_c;
+      c1 = c1 > 0 ? c1 - 1 : 0;
+      if (c1 >= xw.nrows_c) c1 = xw.nrows_c ? xw.nrows_c - 1 : 0;
+      const long long r0 = xw.rowmap ? xw.rowmap[c0] : c0, r1 = xw.rowmap ? xw.rowmap[c1] : c1;
+      UIN used = 0;
+#pragma unroll
+      for (int k = 0; k < sss::XW_MAX; k++) {
+        long long lo = r0 + xw.off[k] - xw.half[k], hi = r1 + xw.off[k] + xw.half[k] + 1;
+        lo = lo < 0 ? 0 : lo;
+        hi = hi > (long long)xw.n ? (long long)xw.n : hi;
+        long long len = (k < xw.nwin && hi > lo) ? hi - lo : 0;
+        if (len > (long long)(xw.cap - used)) len = xw.cap - used;  // shared memory budget
+        sw.lo[k] = lo;
+        sw.len[k] = (UIN)len;
+        sw.base[k] = used;
+        used += (UIN)len;
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < sss::XW_MAX; k++) {
+      const UIN lo = (UIN)sw.lo[k], len = sw.len[k], base = sw.base[k];
+      if (k < NW) {
+        w.lo[k] = lo;
+        w.len[k] = len;
+        w.delta[k] = base - lo;
+      }
+      for (UIN i = threadIdx.x; i < len; i += WARPS * 32) sx[base + i] = __ldg(x + lo + i);
+    }
+    __syncthreads();
+  }
+  if (segid >= nseg) return;
+  const uint32_t sxa = tma::smem_addr(sx);
+  const size_t s0 = segid * seg_slots;
+  const size_t s1 = min(s0 + seg_slots, nslots_pad);
+  const int nbat = (int)((s1 - s0) / BT);
+  sss::Run st;
+  sss::begin(st, o, segid, segh[segid], __ldg(heads + (s0 >> 5)));
+  for (int j = 0; j < nbat; j++) {
+    const size_t b = s0 + (size_t)j * BT;
+    Vals<VT, SPL> v;
+    v.get(val, b, lane);
+    Cols<SPL> c;
+    c.get(col, b, lane);
+    const unsigned bits = (__ldg(heads + (b >> 5) + ((SPL * lane) >> 5)) >> ((SPL * lane) & 31u)) & MASK;
+    double xv[SPL];
+#pragma unroll
+    for (int k = 0; k < SPL; k++) xv[k] = gather<NW>(w, sxa, x, c[k]);
+    VT vv[SPL];
+#pragma unroll
+    for (int k = 0; k < SPL; k++) vv[k] = v[k];
+    const size_t sl = b + (size_t)SPL * lane;
+    if (sl + SPL > nslots) {  // the stream's zero padding adds nothing, whatever x holds
+#pragma unroll
+      for (int k = 0; k < SPL; k++)
+        if (sl + k >= nslots) xv[k] = 0.0;
+    }
+    batch<VT, SPL, BUF>(vv, xv, bits, st, o, rbuf);
+  }
+  sss::finish(st, o);
+}
+
+// Bytes of one stage (one batch of 32*SPL slots: values, columns, bitmap)
+// and of the dynamic shared memory of stream_wide_tma.
+template <typename VT, int SPL>
+constexpr uint32_t stage_bytes() {
+  return 32u * SPL * (uint32_t)sizeof(VT) + 32u * SPL * 4u + 4u * SPL;
+}
+template <typename VT, int SPL, int STAGES, int WARPS, bool BUF>
+constexpr size_t tma_smem_bytes() {
+  return ((WARPS * STAGES * 8 + 127) / 128) * 128 + (size_t)WARPS * STAGES * stage_bytes<VT, SPL>() +
+         (BUF ? (size_t)WARPS * 32 * SPL * sizeof(double) : 0);
+}
+
+// Staged form: persistent warps; warp g of G takes segments g, g + G, ...
+// Lane 0 keeps the warp's next STAGES batches in flight as three bulk
+// copies each (values, columns, bitmap words) completing on the stage's
+// mbarrier.  Waits are bounded: a wait that gives up records
+// ISPMV_ERR_TIMEOUT in *status, the warp stops, and lane 0 waits (bounded)
+// for its copies still in flight before the CTA exits.
+template <typename VT, int SPL, int STAGES, int WARPS, bool BUF>
+__global__ void __launch_bounds__(WARPS * 32)
+    stream_wide_tma(size_t nslots, size_t nslots_pad, size_t seg_slots, size_t nseg, const VT *__restrict__ val,
+                    const UIN *__restrict__ col, const UIN *__restrict__ heads, const UIN *__restrict__ segh,
+                    const FPT *__restrict__ x, seg::Out o, int *status) {
+  constexpr int BT = 32 * SPL;
+  constexpr unsigned MASK = SPL == 32 ? 0xffffffffu : (1u << SPL) - 1u;
+  constexpr uint32_t VB = BT * sizeof(VT), CB = BT * 4, HB = BT / 8, STB = stage_bytes<VT, SPL>();
+  static_assert(VB % 16 == 0 && CB % 16 == 0 && HB % 16 == 0, "bulk copies move multiples of 16 bytes");
+  extern __shared__ __align__(128) unsigned char smem[];
+  const int wib = threadIdx.x >> 5;
+  const unsigned lane = threadIdx.x & 31u;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem) + wib * STAGES;
+  unsigned char *ring = smem + ((WARPS * STAGES * 8 + 127) / 128) * 128 + (size_t)wib * STAGES * STB;
+  double *rbuf = reinterpret_cast<double *>(smem + ((WARPS * STAGES * 8 + 127) / 128) * 128 +
+                                            (size_t)WARPS * STAGES * STB) +
+                 (size_t)wib * BT;
+  const size_t gw = (size_t)blockIdx.x * WARPS + wib, GW = (size_t)gridDim.x * WARPS;
+  if (gw >= nseg) return;
+  if (lane == 0) {
+    for (int s = 0; s < STAGES; s++) tma::bar_init(&bars[s], 1);
+    tma::fence_barrier_init();
+  }
+  __syncwarp();
+  const uint64_t pol = tma::policy_evict_first();
+  // producer position (lane 0): segment and batch of the next copy
+  size_t pseg = gw;
+  uint32_t pbat = 0;
+  auto issue = [&](int s) {
+    const size_t b = pseg * seg_slots + (size_t)pbat * BT;
+    unsigned char *dst = ring + (size_t)s * STB;
+    tma::bar_expect_tx(&bars[s], VB + CB + HB);
+    tma::bulk_g2s(dst, val + b, VB, &bars[s], pol);
+    tma::bulk_g2s(dst + VB, col + b, CB, &bars[s], pol);
+    tma::bulk_g2s(dst + VB + CB, heads + b / 32, HB, &bars[s], pol);
+    if (++pbat >= sss::seg_nst<BT>(pseg, seg_slots, nslots_pad)) {
+      pseg += GW;
+      pbat = 0;
+    }
+  };
+  int inflight = 0;  // copies issued and not yet consumed (lane 0's count)
+  if (lane == 0)
+    for (int s = 0; s < STAGES && pseg < nseg; s++) {
+      issue(s);
+      inflight++;
+    }
+  size_t cseg = gw;
+  uint32_t cbat = 0, t = 0;
+  sss::Run st;
+  bool gaveup = false;
+  while (cseg < nseg) {
+    const int s = (int)(t % STAGES);
+    // the lanes poll independently; they stop together if any gave up
+    if (!__all_sync(FULL, tma::bar_wait(&bars[s], (t / STAGES) & 1u))) {
+      if (lane == 0 && status) atomicCAS(status, 0, ISPMV_ERR_TIMEOUT);
+      gaveup = true;
+      break;
+    }
+    const unsigned char *stage = ring + (size_t)s * STB;
+    const size_t b = cseg * seg_slots + (size_t)cbat * BT;
+    const UIN *shd = reinterpret_cast<const UIN *>(stage + VB + CB);
+    if (cbat == 0) sss::begin(st, o, cseg, segh[cseg], shd[0]);
+    const unsigned bits = (shd[(SPL * lane) >> 5] >> ((SPL * lane) & 31u)) & MASK;
+    UIN c[SPL];
+#pragma unroll
+    for (int i = 0; i < SPL / 4; i++) {
+      const uint4 q = *reinterpret_cast<const uint4 *>(stage + VB + 16u * (32u * i + lane));
+      c[4 * i] = q.x;
+      c[4 * i + 1] = q.y;
+      c[4 * i + 2] = q.z;
+      c[4 * i + 3] = q.w;
+    }
+    double xv[SPL];
+#pragma unroll
+    for (int k = 0; k < SPL; k++) xv[k] = __ldg(x + c[k]);
+    VT v[SPL];
+    if constexpr (sizeof(VT) == 8) {
+#pragma unroll
+      for (int i = 0; i < SPL / 2; i++) {
+        const double2 q = *reinterpret_cast<const double2 *>(stage + 16u * (32u * i + lane));
+        v[2 * i] = q.x;
+        v[2 * i + 1] = q.y;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < SPL / 4; i++) {
+        const float4 q = *reinterpret_cast<const float4 *>(stage + 16u * (32u * i + lane));
+        v[4 * i] = q.x;
+        v[4 * i + 1] = q.y;
+        v[4 * i + 2] = q.z;
+        v[4 * i + 3] = q.w;
+      }
+    }
+    // every lane has read the stage: refill it with the batch STAGES ahead
+    __syncwarp();
+    if (lane == 0) {
+      inflight--;
+      if (pseg < nseg) {
+        tma::fence_proxy_async();
+        issue(s);
+        inflight++;
+      }
+    }
+    const size_t sl = b + (size_t)SPL * lane;
+    if (sl + SPL > nslots) {  // the stream's zero padding adds nothing, whatever x holds
+#pragma unroll
+      for (int k = 0; k < SPL; k++)
+        if (sl + k >= nslots) xv[k] = 0.0;
+    }
+    batch<VT, SPL, BUF>(v, xv, bits, st, o, rbuf);
+    if (++cbat >= sss::seg_nst<BT>(cseg, seg_slots, nslots_pad)) {
+      sss::finish(st, o);
+      cseg += GW;
+      cbat = 0;
+    }
+    t++;
+  }
+  if (gaveup && lane == 0) {
+    // the copies still in flight complete on the next phases of their stages
+    for (int i = 0; i < inflight; i++) {
+      const uint32_t tt = t + (uint32_t)i;
+      (void)tma::bar_wait(&bars[tt % STAGES], (tt / STAGES) & 1u);
+    }
+  }
+}
+
+}  // namespace wide
+}  // namespace ispmv

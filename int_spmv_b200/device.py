@@ -88,7 +88,8 @@ def int_axt_com_h1(bn, bs, log, thw, tn, lenAX, lenRWP, ax, rwp, y, stream=None)
 
 VAL_KINDS = {"f64": abi.VAL_F64, "f32": abi.VAL_F32, "f32lo": abi.VAL_F32_LO16}
 COL_KINDS = {"u32": abi.COL_U32, "d16": abi.COL_D16}
-KERNELS = {"auto": abi.KERNEL_AUTO, "ldg": abi.KERNEL_LDG, "tma": abi.KERNEL_TMA, "rows": abi.KERNEL_ROWS}
+KERNELS = {"auto": abi.KERNEL_AUTO, "ldg": abi.KERNEL_LDG, "tma": abi.KERNEL_TMA, "rows": abi.KERNEL_ROWS,
+           "wide": abi.KERNEL_WIDE}
 
 
 def plan_opts(val="f64", col="u32", kernel="auto", units_per_warp=0, ctas_per_sm=0, lo_tol=0.0,

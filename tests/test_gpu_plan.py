@@ -18,8 +18,10 @@ pytestmark = pytest.mark.gpu
 COMBOS = [("CSR", "rows"), ("CSR", "ldg"), ("CSR", "tma"), ("AXC", "rows"), ("AXC", "ldg"), ("AXC", "tma"),
           ("K1", "auto"), ("K1P", "auto"), ("NOC1", "ldg"), ("NOC1", "tma"), ("NOC4", "ldg"), ("NOC4", "tma"),
           ("NOC8", "ldg"), ("NOC8", "tma"), ("NOC16", "ldg"), ("NOC16", "tma"), ("NOC3", "ldg"),
-          ("COM128", "ldg"), ("COM128", "tma"), ("COM256", "ldg"), ("COM512", "tma")]
-KIDS = {"ldg": 1, "tma": 2, "rows": 3}
+          ("COM128", "ldg"), ("COM128", "tma"), ("COM256", "ldg"), ("COM512", "tma"),
+          ("COM128", "wide"), ("NOC1", "wide"), ("AXC", "wide"), ("CSR", "wide")]
+KIDS = {"ldg": 1, "tma": 2, "rows": 3, "wide": 4}
+WIDE_VARIANTS = list(range(14))
 
 
 @pytest.fixture(scope="module")
@@ -120,8 +122,40 @@ def test_xband_variants(env, case, variant):
         check_plan(env, row, col, val, x, fmt, kernel="ldg", variant=variant)
 
 
+@pytest.mark.parametrize("fmt", ["COM128", "NOC1", "AXC", "CSR"])
+@pytest.mark.parametrize("variant", WIDE_VARIANTS)
+@pytest.mark.parametrize("val_kind", ["f64", "f32"])
+def test_wide_variants(env, fmt, variant, val_kind):
+    """The lane-interleaved kernel (8 or 16 slots per lane, with and without
+    shared-memory x bands) on random rows, long rows spanning segments, a
+    banded matrix with empty rows and a 27-point stencil (three bands)."""
+    from int_spmv_b200 import matrices as M
+    mats = [M.random_csr(7001, 12, rl_max=90, empty_frac=0.1), M.random_csr(3001, 9, rl_max=700, empty_frac=0.2),
+            M.fem_banded(20011, np.random.default_rng(5), 3, 30), M.stencil27(22, seed=2)]
+    for i, (row, col, val) in enumerate(mats):
+        x = M.uniform_x(len(row) - 1, 12 + i)
+        for beta in (0, 1):
+            p, _ = check_plan(env, row, col, val, x, fmt, val_kind, beta, kernel="wide", variant=variant)
+            assert p.info["kernel"] == 4 and p.kernel_name().startswith("stream_wide")
+
+
+def test_wide_rejects_other_forms(env):
+    torch, D, F, orc = env
+    from int_spmv_b200 import IntSpmvError
+    g = load_golden("random257_empty")
+    csr = F.CSR(g["row"], g["col"], g["val"])
+    with pytest.raises(IntSpmvError):
+        make_plan(F, D, csr, g["x"], "COM128", col="d16", kernel="wide")
+    with pytest.raises(IntSpmvError):
+        make_plan(F, D, csr, g["x"], "COM128", val="f32lo", kernel="wide")
+    p = make_plan(F, D, csr, g["x"], "COM128", kernel="wide")
+    X = torch.zeros((csr.n, 8), dtype=torch.float64, device="cuda")
+    with pytest.raises(IntSpmvError):
+        p.spmm(X)
+
+
 @pytest.mark.parametrize("fmt,kernel", [("NOC1", "ldg"), ("NOC4", "tma"), ("COM128", "ldg"), ("COM128", "tma"),
-                                        ("CSR", "rows"), ("K1P", "auto")])
+                                        ("CSR", "rows"), ("K1P", "auto"), ("COM128", "wide"), ("CSR", "wide")])
 def test_deterministic_and_host_e2e(env, fmt, kernel):
     torch, D, F, orc = env
     from int_spmv_b200 import matrices as M
@@ -144,7 +178,8 @@ def poisson512(env):
     return row, col, val, M.uniform_x(len(row) - 1, 0)
 
 
-@pytest.mark.parametrize("fmt,kernel", [("CSR", "rows"), ("NOC1", "ldg"), ("NOC1", "tma"), ("COM128", "ldg")])
+@pytest.mark.parametrize("fmt,kernel", [("CSR", "rows"), ("NOC1", "ldg"), ("NOC1", "tma"), ("COM128", "ldg"),
+                                        ("NOC1", "wide"), ("COM128", "wide")])
 def test_poisson512(env, poisson512, fmt, kernel):
     row, col, val, x = poisson512
     assert len(row) - 1 == 262144 and len(col) == 1308672
@@ -161,12 +196,12 @@ def powerlaw4m(env):
 @pytest.mark.parametrize("fmt,kernel", [("CSR", "rows"), ("CSR", "ldg"), ("AXC", "rows"), ("AXC", "ldg"),
                                         ("K1P", "auto"), ("NOC1", "ldg"), ("NOC1", "tma"), ("NOC4", "ldg"),
                                         ("NOC4", "tma"), ("NOC8", "tma"), ("COM128", "ldg"), ("COM128", "tma"),
-                                        ("COM512", "ldg")])
+                                        ("COM512", "ldg"), ("COM128", "wide"), ("NOC1", "wide"), ("CSR", "wide")])
 def test_powerlaw_4m(env, powerlaw4m, fmt, kernel):
     row, col, val, x = powerlaw4m
     p, _ = check_plan(env, row, col, val, x, fmt, kernel=kernel)
     assert p.status() == 0
-    if (fmt, kernel) in (("COM128", "ldg"), ("NOC1", "ldg")):
+    if (fmt, kernel) in (("COM128", "ldg"), ("NOC1", "ldg"), ("COM128", "wide")):
         check_plan(env, row, col, val, x, fmt, val_kind="f32", kernel=kernel)
 
 
