@@ -161,6 +161,14 @@ int ispmv_build_axt_cols(UIN ompNT, const str_matCSR *csr, const str_matAXT *axt
  * count+1 entries.  Arrays are malloc'd (ispmv_csr_free); rl and the
  * statistics are filled. */
 int ispmv_csr_blockdiag(UIN count, const str_matCSR *mats, str_matCSR *out, UIN *off);
+/* Seeded banded FEM-like matrix (no reference counterpart; a benchmark
+ * workload generator): row r holds rl uniform in [rl_lo, rl_hi] (at most n)
+ * entries, the diagonal plus rl-1 distinct columns uniform in
+ * [r - band*rl, r + band*rl] clipped to [0, n); off-diagonals N(0,1), the
+ * diagonal |off-diagonal sum| + 1; ascending columns.  Arrays malloc'd
+ * (ispmv_csr_free); rl and statistics filled.  Deterministic in (n, seed,
+ * rl_lo, rl_hi, band) whatever the thread count. */
+int ispmv_gen_banded(UIN n, uint64_t seed, UIN rl_lo, UIN rl_hi, UIN band, str_matCSR *out);
 
 /* Frees the arrays a builder allocated and zeroes the struct. */
 void ispmv_free_axc(str_matAXC *m);
@@ -343,6 +351,12 @@ const char *ispmv_status_string(int status);
 const char *ispmv_last_error(void);
 /* Kernel launches issued by the library since load (all ispmv_* calls). */
 unsigned long long ispmv_launch_count(void);
+
+/* Self-test of the bounded device wait the staged kernels use on their
+ * mbarriers (no reference counterpart): waits on a barrier nothing completes,
+ * and returns ISPMV_ERR_TIMEOUT when the wait gave up after its limit (about
+ * 200 ms) as designed; *elapsed_ms = how long the wait took. */
+int ispmv_selftest_bounded_wait(double *elapsed_ms, void *stream);
 
 #ifdef __cplusplus
 }

@@ -68,6 +68,8 @@ P_PLAN = C.POINTER(VP)
 
 # name: (restype, argtypes).  Every `extern "C"` function of include/intspmv.h.
 PROTOTYPES: dict[str, tuple] = {
+    # self-test of the bounded device wait
+    "ispmv_selftest_bounded_wait": (C.c_int, [C.POINTER(C.c_double), C.c_void_p]),
     # host: statistics, files, builders
     "ispmv_csr_stats": (C.c_int, [P_CSR]),
     "printMatrixStats": (None, [C.c_char_p, P_CSR]),
@@ -86,6 +88,7 @@ PROTOTYPES: dict[str, tuple] = {
     "ispmv_build_axc_cols": (C.c_int, [UIN, P_CSR, P_AXC, P_P_UIN]),
     "ispmv_build_axt_cols": (C.c_int, [UIN, P_CSR, P_AXT, P_P_UIN]),
     "ispmv_csr_blockdiag": (C.c_int, [UIN, P_CSR, P_CSR, P_UIN]),
+    "ispmv_gen_banded": (C.c_int, [UIN, C.c_uint64, UIN, UIN, UIN, P_CSR]),
     "ispmv_free_axc": (None, [P_AXC]),
     "ispmv_free_k1": (None, [P_K1]),
     "ispmv_free_axt": (None, [P_AXT]),

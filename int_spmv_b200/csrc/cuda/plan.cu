@@ -57,6 +57,7 @@ struct ispmv_plan_s {
   double lo_frac = 0.0;   // fraction of slots carrying a lo-word
   size_t esc_batches = 0; // D16 batches kept as u32 columns
   FPT *hx = nullptr, *hy = nullptr;  // device staging of ispmv_plan_spmv_host
+  float *x32 = nullptr;              // FP32 copy of x (FP32-value stream_wide plans)
   unsigned long long *queue = nullptr;  // work-queue counter (variant ISPMV_VARIANT_QUEUE)
   cudaStream_t cap_stream = nullptr;    // private stream for graph capture
   cudaGraph_t graph = nullptr;
@@ -247,6 +248,8 @@ WideCfg wide_variant(int v) {
     case 11: return {16, false, 0, 4096, 0, false, true, 2, 4};
     case 12: return {16, false, 0, 4096, 0, false, true, 3, 4};
     case 13: return {8, false, 0, 4096, 0, false, true, 4, 4};
+    case 14: return {16, false, 0, 4096, 2, false, false, 0, 8};
+    case 15: return {16, false, 0, 8192, 2, false, false, 0, 8};
     default: return {16, false, 0, 4096, 3, false, false, 0, 8};
   }
 }
@@ -580,7 +583,16 @@ ISPMV_API int ispmv_plan_axt(const str_matCSR *csr, const str_matAXT *axt, const
     for (size_t q = 0; q < p->slots; q++) v[q] = axt->ax[(q / 8) * 16 + q % 8];
     std::vector<size_t> start(p->n);
     for (UIN r = 0; r < p->n; r++) start[r] = (size_t)(axt->con[r] / 16) * 8 + axt->con[r] % 16;
-    if (p->opts.kernel == ISPMV_KERNEL_AUTO) p->opts.kernel = ISPMV_KERNEL_LDG;
+    if (p->opts.kernel == ISPMV_KERNEL_AUTO) {
+      // the lane-interleaved kernel where it takes the value/column forms;
+      // 16 slots per lane for rows of 16 slots or more on average, else 8
+      if (narrow_kinds(p)) {
+        p->opts.kernel = ISPMV_KERNEL_LDG;
+      } else {
+        p->opts.kernel = ISPMV_KERNEL_WIDE;
+        if (p->opts.variant == 0) p->opts.variant = (double)p->slots >= 16.0 * (double)p->n ? 0 : 4;
+      }
+    }
     st = setup_stream(p, csr, v, c, start);
   } else {
     // tile columns: the unit engine on the reference's per-column rows
@@ -659,7 +671,22 @@ int launch_staged_w(K kernel, size_t smem, size_t nseg, int ctas_per_sm, cudaStr
 
 template <typename VT, int SPL, int NW, int MINB, bool BUF>
 int launch_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, const char *name) {
-  auto *k = wide::stream_wide<VT, SPL, NW, WIDE_WARPS, MINB, BUF>;
+  if constexpr (sizeof(VT) == 4 && NW == 0) {
+    // FP32 values: gather from an FP32 copy of x (the value the FP32 multiply uses)
+    if (!p->x32) TRY(dev_alloc(p, p->n, &p->x32));
+    const unsigned gc = (unsigned)std::min<size_t>(((size_t)p->n / 2 + 255) / 256, (size_t)sm_count() * 8) + 1;
+    if ((reinterpret_cast<uintptr_t>(x) & 15u) == 0) wide::x_to_f32<true><<<gc, 256, 0, s>>>(p->n, x, p->x32);
+    else wide::x_to_f32<false><<<gc, 256, 0, s>>>(p->n, x, p->x32);
+    TRY(check_launch("x_to_f32"));
+    auto *k = wide::stream_wide<VT, float, SPL, NW, WIDE_WARPS, MINB, BUF>;
+    const size_t smem = (BUF ? (size_t)WIDE_WARPS * 32 * SPL : 0) * sizeof(double);
+    if (smem) ISPMV_TRY(cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<(unsigned)((p->nseg + WIDE_WARPS - 1) / WIDE_WARPS), WIDE_WARPS * 32, smem, s>>>(
+        p->slots, p->slots_pad, p->seg_slots, p->nseg, static_cast<const VT *>(p->val), p->col, p->heads, p->segh,
+        p->xw, p->x32, o);
+    return check_launch(name);
+  }
+  auto *k = wide::stream_wide<VT, double, SPL, NW, WIDE_WARPS, MINB, BUF>;
   const size_t smem =
       ((NW ? (size_t)p->xw.cap : 0) + (BUF ? (size_t)WIDE_WARPS * 32 * SPL : 0)) * sizeof(double);
   if (smem) ISPMV_TRY(cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -711,7 +738,7 @@ int run_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
     if (wc.buf) { ISPMV_WIDE_NW(8, 4, 1) }
     ISPMV_WIDE_NW(8, 4, 0)
   }
-  if (wc.win) {
+  if (wc.minb == 2) {
     if (wc.buf) { ISPMV_WIDE_NW(16, 2, 1) }
     ISPMV_WIDE_NW(16, 2, 0)
   }
@@ -1043,6 +1070,11 @@ ISPMV_API int ispmv_plan_spmv_host(ispmv_plan p, const FPT *h_x, FPT *h_y, void 
 }
 
 namespace {
+// Slots per lane of a lane-interleaved (stream_wide) plan, 0 for slot order.
+unsigned il_spl(const ispmv_plan_s *p) {
+  return p->opts.kernel == ISPMV_KERNEL_WIDE ? (unsigned)wide_variant(p->opts.variant).spl : 0u;
+}
+
 template <int G, typename VT>
 int spmm_blocks(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
   constexpr int NG = 32 / G;
@@ -1057,7 +1089,7 @@ int spmm_blocks(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
     mm::Out o{Y, p->rowmap, p->mm_row, p->mm_sum, k, j0, std::min<UIN>(G, k - j0)};
     const unsigned g = (unsigned)((p->nseg * 32 + 255) / 256);
     mm::stream_spmm<G, VT><<<g, 256, 0, s>>>(p->slots, p->slots_pad, p->seg_slots, p->nseg, val, p->col, p->heads,
-                                             p->segh, X, o);
+                                             p->segh, X, o, il_spl(p));
     TRY(check_launch("stream_spmm"));
     const size_t work = std::max(nrec, p->nempty) * G;
     mm::spmm_fixup<G><<<(unsigned)((work + 255) / 256), 256, 0, s>>>(nrec, p->mm_row, p->mm_sum, p->empty,
@@ -1081,8 +1113,8 @@ int spmm_run(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
 // (AXT COM, AXT tileH=1, AXC and CSR built with the stream kernels).
 ISPMV_API int ispmv_plan_spmm(ispmv_plan p, UIN k, const FPT *X, FPT *Y, void *stream) {
   if (!p || !X || !Y || k == 0) return ISPMV_ERR_ARG;
-  if (p->path != P_STREAM || narrow_kinds(p) || p->opts.kernel == ISPMV_KERNEL_WIDE)
-    return fail(ISPMV_ERR_UNSUPPORTED, "ispmv_plan_spmm: needs a slot-stream plan with u32 columns in slot order");
+  if (p->path != P_STREAM || narrow_kinds(p))
+    return fail(ISPMV_ERR_UNSUPPORTED, "ispmv_plan_spmm: needs a slot-stream plan with u32 columns");
   cudaStream_t s = as_stream(stream);
   if (!p->slots) {  // every row empty
     ISPMV_TRY(cudaMemsetAsync(Y, 0, (size_t)p->n * k * sizeof(FPT), s));

@@ -9,9 +9,11 @@
 // a contiguous row piece of X) and accumulates.  Row starts come from the
 // stream's bitmap; a row that ends inside the group's part is written to Y
 // directly, the runs open at the part's two ends become G-wide records that
-// spmm_fixup adds per row.  Deterministic, no atomics.
+// spmm_fixup adds per row.  Deterministic, no atomics.  `il_spl` > 0 reads
+// a plan whose values and columns are stored lane-interleaved for
+// stream_wide (wide::il_pos with il_spl slots per lane).
 #pragma once
-#include "sss.cuh"
+#include "wide.cuh"
 
 namespace ispmv {
 namespace mm {
@@ -30,7 +32,7 @@ template <int G, typename VT>
 __global__ void __launch_bounds__(256) stream_spmm(size_t nslots, size_t nslots_pad, size_t seg_slots, size_t nseg,
                                                    const VT *__restrict__ val, const UIN *__restrict__ col,
                                                    const UIN *__restrict__ heads, const UIN *__restrict__ segh,
-                                                   const FPT *__restrict__ X, Out o) {
+                                                   const FPT *__restrict__ X, Out o, unsigned il_spl) {
   constexpr int NG = 32 / G;  // groups per warp = parts per segment
   const unsigned lane = threadIdx.x & 31u, grp = lane / G, j = lane % G;
   const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (grp * G));
@@ -62,8 +64,8 @@ __global__ void __launch_bounds__(256) stream_spmm(size_t nslots, size_t nslots_
   for (size_t c0 = a; c0 < b; c0 += G) {
     // one slot per lane of the group, broadcast below
     const size_t my = c0 + j;
-    const VT mv = val[my];
-    const UIN mc = col[my];
+    const VT mv = val[il_spl ? wide::il_pos(my, il_spl, 16u / sizeof(VT)) : my];
+    const UIN mc = col[il_spl ? wide::il_pos(my, il_spl, 4u) : my];
     const UIN hw = __ldg(heads + (c0 >> 5));
 #pragma unroll 4
     for (int i = 0; i < G; i++) {

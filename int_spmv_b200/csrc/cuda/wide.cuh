@@ -83,6 +83,34 @@ struct Cols {
   }
 };
 
+// acc + v*x in the plan's value form: FP64 values fused multiply-add; FP32
+// values multiplied in FP32 (x rounded to FP32, or gathered from the plan's
+// FP32 copy of x, the same value) and added in FP64.
+__device__ __forceinline__ double madd(double v, double x, double acc) { return fma(v, x, acc); }
+__device__ __forceinline__ double madd(float v, double x, double acc) {
+  return acc + (double)(v * __double2float_rn(x));
+}
+__device__ __forceinline__ double madd(float v, float x, double acc) { return acc + (double)(v * x); }
+
+// x rounded to FP32 once per product, for FP32-value plans: their gathers
+// then move 4 bytes per slot and an L1 line serves 32 columns.  VEC: x and
+// x32 are 16- and 8-byte aligned, two elements per thread and step.
+template <bool VEC>
+__global__ void __launch_bounds__(256) x_to_f32(size_t n, const FPT *__restrict__ x, float *__restrict__ x32) {
+  const size_t stride = (size_t)gridDim.x * 256;
+  size_t i = (size_t)blockIdx.x * 256 + threadIdx.x;
+  if constexpr (VEC) {
+    const size_t n2 = n / 2;
+    for (; i < n2; i += stride) {
+      const double2 v = __ldcs(reinterpret_cast<const double2 *>(x) + i);
+      reinterpret_cast<float2 *>(x32)[i] = make_float2(__double2float_rn(v.x), __double2float_rn(v.y));
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && (n & 1)) x32[n - 1] = __double2float_rn(x[n - 1]);
+  } else {
+    for (; i < n; i += stride) x32[i] = __double2float_rn(__ldg(x + i));
+  }
+}
+
 // The bands of x a CTA stages: band k holds columns [lo[k], lo[k] + len[k])
 // at shared-memory offset lo[k] + delta[k] (u32 arithmetic, modulo 2^32).
 template <int NW>
@@ -136,27 +164,31 @@ __device__ __forceinline__ double gather(const Bands<NW> &w, uint32_t sx_addr, c
 // open at the batch start, entry i the row of the batch's i-th start.  The
 // warp then stores the entries to y with coalesced stores.  !BUF: every row
 // goes to y (or to the segment's head record) from the lane that ends it.
-template <typename VT, int SPL, bool BUF>
-__device__ __forceinline__ void batch(const VT (&v)[SPL], const double (&xv)[SPL], unsigned bits, sss::Run &st,
+template <typename VT, typename XT, int SPL, bool BUF>
+__device__ __forceinline__ void batch(const VT (&v)[SPL], const XT (&xv)[SPL], unsigned bits, sss::Run &st,
                                       const seg::Out &o, double *rbuf) {
   const unsigned lane = threadIdx.x & 31u;
   const unsigned cnt = __popc(bits);
-  unsigned incl = cnt;  // row starts up to and including my slots
+  // row starts before my slots (ex) and in the batch (tot): counts summed
+  // bit plane by bit plane with ballots, keeping the shuffle (LSU) pipe free
+  constexpr int PLANES = SPL >= 16 ? 5 : SPL >= 8 ? 4 : 3;
+  const unsigned lt = sss::lanemask_le() >> 1;  // lanes below mine
+  unsigned ex = 0, tot = 0;
 #pragma unroll
-  for (int d = 1; d < 32; d <<= 1) {
-    const unsigned t = __shfl_up_sync(FULL, incl, d);
-    if ((int)lane >= d) incl += t;
+  for (int q = 0; q < PLANES; q++) {
+    const unsigned m = __ballot_sync(FULL, (cnt >> q) & 1u);
+    ex += (unsigned)__popc(m & lt) << q;
+    tot += (unsigned)__popc(m) << q;
   }
-  const unsigned tot = __shfl_sync(FULL, incl, 31);
-  const unsigned ex = incl - cnt;   // entry of the row open at my first slot
+  // ex = entry of the row open at my first slot
   const UIN rb = st.rbase + ex;     // row of my first start
   const int first = cnt ? __ffs(bits) - 1 : SPL;
   double pre = 0.0, acc = 0.0;
   if (__all_sync(FULL, cnt <= 1u)) {
 #pragma unroll
     for (int k = 0; k < SPL; k++) {
-      if (k < first) pre = pk::fmac<VT>(v[k], xv[k], pre);
-      else acc = pk::fmac<VT>(v[k], xv[k], acc);
+      if (k < first) pre = madd(v[k], xv[k], pre);
+      else acc = madd(v[k], xv[k], acc);
     }
   } else {
     UIN r = rb;        // row of the run being summed, once past my first start
@@ -177,7 +209,7 @@ __device__ __forceinline__ void batch(const VT (&v)[SPL], const double (&xv)[SPL
         e++;
         acc = 0.0;
       }
-      acc = pk::fmac<VT>(v[k], xv[k], acc);
+      acc = madd(v[k], xv[k], acc);
     }
     if (!cnt) {
       pre = acc;
@@ -232,11 +264,12 @@ __device__ __forceinline__ void batch(const VT (&v)[SPL], const double (&xv)[SPL
 // registers.  NW = number of shared-memory x bands (0: every gather through
 // L1/L2).  Dynamic shared memory: xw.cap doubles of bands (NW > 0), then
 // (BUF) WARPS row buffers of 32*SPL doubles.
-template <typename VT, int SPL, int NW, int WARPS, int MINB, bool BUF>
+template <typename VT, typename XT, int SPL, int NW, int WARPS, int MINB, bool BUF>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
     stream_wide(size_t nslots, size_t nslots_pad, size_t seg_slots, size_t nseg, const VT *__restrict__ val,
                 const UIN *__restrict__ col, const UIN *__restrict__ heads, const UIN *__restrict__ segh,
-                sss::XWin xw, const FPT *__restrict__ x, seg::Out o) {
+                sss::XWin xw, const XT *__restrict__ x, seg::Out o) {
+  static_assert(NW == 0 || sizeof(XT) == 8, "shared-memory x bands hold FP64 x");
   constexpr int BT = 32 * SPL;
   constexpr unsigned MASK = SPL == 32 ? 0xffffffffu : (1u << SPL) - 1u;
   extern __shared__ __align__(16) double sx[];
@@ -298,9 +331,12 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
     Cols<SPL> c;
     c.get(col, b, lane);
     const unsigned bits = (__ldg(heads + (b >> 5) + ((SPL * lane) >> 5)) >> ((SPL * lane) & 31u)) & MASK;
-    double xv[SPL];
+    XT xv[SPL];
 #pragma unroll
-    for (int k = 0; k < SPL; k++) xv[k] = gather<NW>(w, sxa, x, c[k]);
+    for (int k = 0; k < SPL; k++) {
+      if constexpr (NW > 0) xv[k] = gather<NW>(w, sxa, x, c[k]);
+      else xv[k] = __ldg(x + c[k]);
+    }
     VT vv[SPL];
 #pragma unroll
     for (int k = 0; k < SPL; k++) vv[k] = v[k];
@@ -308,9 +344,9 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
     if (sl + SPL > nslots) {  // the stream's zero padding adds nothing, whatever x holds
 #pragma unroll
       for (int k = 0; k < SPL; k++)
-        if (sl + k >= nslots) xv[k] = 0.0;
+        if (sl + k >= nslots) xv[k] = (XT)0;
     }
-    batch<VT, SPL, BUF>(vv, xv, bits, st, o, rbuf);
+    batch<VT, XT, SPL, BUF>(vv, xv, bits, st, o, rbuf);
   }
   sss::finish(st, o);
 }
@@ -442,7 +478,7 @@ __global__ void __launch_bounds__(WARPS * 32)
       for (int k = 0; k < SPL; k++)
         if (sl + k >= nslots) xv[k] = 0.0;
     }
-    batch<VT, SPL, BUF>(v, xv, bits, st, o, rbuf);
+    batch<VT, double, SPL, BUF>(v, xv, bits, st, o, rbuf);
     if (++cbat >= sss::seg_nst<BT>(cseg, seg_slots, nslots_pad)) {
       sss::finish(st, o);
       cseg += GW;

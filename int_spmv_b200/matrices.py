@@ -182,6 +182,39 @@ def fem_batch(count: int = 512, seed: int = 4, n_lo: float = 1e3, n_hi: float = 
     return [fem_banded(int(k), rng) for k in ns]
 
 
+def fem_banded_c(n: int, seed: int, rl_lo: int = 7, rl_hi: int = 81, band: int = 3):
+    """The banded FEM-like matrix of fem_banded (same distribution: rl
+    uniform in [rl_lo, rl_hi], rl-1 distinct columns uniform within +/-band*rl
+    of the diagonal, N(0,1) off-diagonals, diagonal |row sum| + 1) from the
+    library's seeded C generator (ispmv_gen_banded: OpenMP over rows,
+    SplitMix64 streams per row), fast enough for the full batched workload
+    (about 1e9 nonzeros).  Its random stream differs from fem_banded's."""
+    import ctypes as C
+
+    from . import abi
+    from ._lib import check, load
+    lib = load()
+    out = abi.StrMatCSR()
+    check(lib.ispmv_gen_banded(n, seed, rl_lo, rl_hi, band, C.byref(out)), "ispmv_gen_banded")
+    try:
+        nnz = out.nnz
+        row = np.ctypeslib.as_array(out.row, shape=(n + 1,)).copy()
+        col = np.ctypeslib.as_array(out.col, shape=(max(nnz, 1),))[:nnz].copy()
+        val = np.ctypeslib.as_array(out.val, shape=(max(nnz, 1),))[:nnz].copy()
+    finally:
+        lib.ispmv_csr_free(C.byref(out))
+    return row, col, val
+
+
+def fem_batch_c(count: int = 512, seed: int = 4, n_lo: float = 1e3, n_hi: float = 2e5):
+    """`count` banded FEM-like matrices with n log-uniform in [n_lo, n_hi]
+    (the sizes of fem_batch for the same seed), each from fem_banded_c with
+    seed (seed, m)."""
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(np.log(n_lo), np.log(n_hi), count)).astype(np.int64)
+    return [fem_banded_c(int(k), seed * 1_000_003 + m) for m, k in enumerate(ns)]
+
+
 def uniform_x(n: int, seed: int, k: int | None = None) -> np.ndarray:
     """x ~ U[-1, 1] (FP64), or an n x k row-major block of them."""
     rng = np.random.default_rng(seed)

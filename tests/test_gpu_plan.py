@@ -21,7 +21,7 @@ COMBOS = [("CSR", "rows"), ("CSR", "ldg"), ("CSR", "tma"), ("AXC", "rows"), ("AX
           ("COM128", "ldg"), ("COM128", "tma"), ("COM256", "ldg"), ("COM512", "tma"),
           ("COM128", "wide"), ("NOC1", "wide"), ("AXC", "wide"), ("CSR", "wide")]
 KIDS = {"ldg": 1, "tma": 2, "rows": 3, "wide": 4}
-WIDE_VARIANTS = list(range(14))
+WIDE_VARIANTS = list(range(16))
 
 
 @pytest.fixture(scope="module")
@@ -148,10 +148,21 @@ def test_wide_rejects_other_forms(env):
         make_plan(F, D, csr, g["x"], "COM128", col="d16", kernel="wide")
     with pytest.raises(IntSpmvError):
         make_plan(F, D, csr, g["x"], "COM128", val="f32lo", kernel="wide")
-    p = make_plan(F, D, csr, g["x"], "COM128", kernel="wide")
-    X = torch.zeros((csr.n, 8), dtype=torch.float64, device="cuda")
-    with pytest.raises(IntSpmvError):
-        p.spmm(X)
+
+
+@pytest.mark.parametrize("fmt", ["COM128", "NOC1"])
+def test_auto_picks_wide(env, fmt):
+    """AXT COM and tileH=1 plans default to the lane-interleaved kernel: 16
+    slots per lane for long rows, 8 for short; narrow forms keep stream_ldg."""
+    torch, D, F, orc = env
+    from int_spmv_b200 import matrices as M
+    for rl_max, spl in ((8, "<8,"), (60, "<16,")):
+        row, col, val = M.random_csr(5000, rl_max, rl_max=rl_max, empty_frac=0.05)
+        x = M.uniform_x(5000, rl_max)
+        p, _ = check_plan(env, row, col, val, x, fmt)
+        assert p.info["kernel"] == 4 and p.kernel_name().startswith("stream_wide" + spl)
+        p, _ = check_plan(env, row, col, val, x, fmt, col="d16")
+        assert p.info["kernel"] == 1
 
 
 @pytest.mark.parametrize("fmt,kernel", [("NOC1", "ldg"), ("NOC4", "tma"), ("COM128", "ldg"), ("COM128", "tma"),

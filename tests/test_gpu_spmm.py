@@ -11,7 +11,8 @@ from test_gpu_plan import make_plan
 
 pytestmark = pytest.mark.gpu
 
-STREAM = [("COM128", "ldg"), ("NOC1", "ldg"), ("AXC", "ldg"), ("CSR", "ldg"), ("COM512", "tma")]
+STREAM = [("COM128", "ldg"), ("NOC1", "ldg"), ("AXC", "ldg"), ("CSR", "ldg"), ("COM512", "tma"), ("COM128", "wide"),
+          ("NOC1", "wide"), ("COM256", "auto")]
 
 
 @pytest.fixture(scope="module")

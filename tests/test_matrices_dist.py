@@ -93,3 +93,41 @@ def test_max_over_ranks_gloo():
     for p in ps:
         p.join(timeout=60)
     assert res == {0: 3.5, 1: 3.5}
+
+
+def test_gen_banded_invariants():
+    """The C generator of the batched workload: row lengths, band, distinct
+    ascending columns with the diagonal, diagonal = |off-diagonal sum| + 1,
+    N(0,1) off-diagonals, and determinism."""
+    from int_spmv_b200 import matrices as M
+    for n, seed in ((1, 3), (9, 4), (1000, 5), (20011, 6)):
+        row, col, val = M.fem_banded_c(n, seed)
+        rl = np.diff(row.astype(np.int64))
+        assert np.all(rl >= min(7, n)) and np.all(rl <= min(81, n))
+        rows = np.repeat(np.arange(n), rl)
+        assert np.all(np.abs(col.astype(np.int64) - rows) <= 3 * rl[rows])
+        # ascending, distinct within each row
+        d = np.diff(col.astype(np.int64))
+        inner = np.ones(len(col), bool)
+        inner[row[1:-1].astype(np.int64)] = False
+        assert np.all(d[inner[1:]] > 0)
+        diag = col.astype(np.int64) == rows
+        assert np.array_equal(np.bincount(rows[diag], minlength=n), np.ones(n, np.int64))
+        offsum = np.bincount(rows[~diag], weights=val[~diag], minlength=n)
+        assert np.allclose(val[diag], np.abs(offsum) + 1.0)
+        r2, c2, v2 = M.fem_banded_c(n, seed)
+        assert np.array_equal(row, r2) and np.array_equal(col, c2) and np.array_equal(val, v2)
+    off = val[~diag]
+    assert abs(off.mean()) < 0.01 and abs(off.std() - 1.0) < 0.01
+    # uniform within the band: the mean offset is near 0 and |offset|/(3*rl) near 1/2
+    offs = (col.astype(np.int64) - rows)[~diag] / (3.0 * rl[rows][~diag])
+    interior = (rows[~diag] > 300) & (rows[~diag] < n - 300)
+    assert abs(offs[interior].mean()) < 0.01 and abs(np.abs(offs[interior]).mean() - 0.5) < 0.01
+
+
+def test_fem_batch_c_sizes_match_fem_batch():
+    from int_spmv_b200 import matrices as M
+    mats = M.fem_batch_c(count=6, seed=4, n_lo=1e3, n_hi=3e3)
+    rng = np.random.default_rng(4)
+    ns = np.exp(rng.uniform(np.log(1e3), np.log(3e3), 6)).astype(np.int64)
+    assert [len(r) - 1 for r, _, _ in mats] == list(ns)
