@@ -251,6 +251,11 @@ def main(argv=None):
     ap.add_argument("--val", default="f64", choices=["f64", "f32", "f32lo"],
                     help="value storage: FP64, or FP32 (+ BF16 lo-word) multiplied in FP32, FP64 accumulation")
     ap.add_argument("--col", default="u32", choices=["u32", "d16"], help="column storage: u32 or 16-bit deltas")
+    ap.add_argument("--mode", default="spmv", choices=["spmv", "spmm", "batch"],
+                    help="spmv: one matrix (default); spmm: Y = A X for k right-hand sides; batch: many "
+                         "uneven banded matrices in one graph launch vs one plan per matrix")
+    ap.add_argument("--batch-count", type=int, default=512)
+    ap.add_argument("--batch-nmax", type=float, default=2e5, help="largest n of the batched matrices")
     ap.add_argument("--no-formats", action="store_true", help="skip the per-format table")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of reference CPU work")
@@ -260,6 +265,10 @@ def main(argv=None):
 
     if a.impl == "reference":
         return main_reference(a, rank, ws, W)
+    if a.mode == "spmm":
+        return main_spmm(a, rank, ws, W)
+    if a.mode == "batch":
+        return main_batch(a, rank, ws, W)
 
     import torch
     torch.cuda.set_device(local_rank)
@@ -370,6 +379,40 @@ def main(argv=None):
                 row_["normwise_err"] = float(np.linalg.norm(e_) / np.linalg.norm(yr))
             formats[f"{p.info['name']}/{vk}/{ck}/{kid}"] = row_
             del p
+        # the vendor library on the same CSR, as a comparison row only (never
+        # the product path): torch's CSR matrix-vector product, cuSPARSE SpMV
+        try:
+            A = torch.sparse_csr_tensor(torch.from_numpy(wl["row"].astype(np.int32)).to(dev),
+                                        torch.from_numpy(wl["col"].astype(np.int32)).to(dev),
+                                        torch.from_numpy(wl["val"]).to(dev), size=(n, n))
+            k = max(20, min(a.steps, 400))
+            s_, _ = timed(lambda: torch.mv(A, x), k, 5, ws, stream, dev)
+            t = s_ / k
+            row_ = {"ms": t * 1e3, "gflops": flops / t / 1e9, "gbs": B / t / 1e9, "frac": B / t / 1e9 / peak,
+                    "kernel": "cuSPARSE SpMV via torch.sparse (library comparison, not the product)"}
+            if check is not None:
+                e_ = np.abs(torch.mv(A, x).cpu().numpy() - yr)
+                row_["max_componentwise_err"] = float(np.max(e_ / np.maximum(ab, 1e-300)))
+            formats["cuSPARSE_CSR/f64/i32/library"] = row_
+            del A
+        except Exception as e:  # the comparison row must not sink the run
+            formats["cuSPARSE_CSR/f64/i32/library"] = {"unavailable": str(e)[:120]}
+
+    # format conversion: the host builder (OpenMP, the reference's layout
+    # rules) against the same conversion on the GPU, for the compacted AXT
+    conversion = None
+    if not a.no_formats:
+        try:
+            fd_h, _ = F.getFormatDataAXT(0, 128, 8, 1, "COM", csr, wl["x"])
+            dv = D.DeviceAXT(D.to_device(wl["row"]), D.to_device(wl["col"]), D.to_device(wl["val"]), x,
+                             bs=128, th=1, mode="COM")
+            dv_s = dv.conversion_s
+            del dv
+            conversion = {"format": "AXT_COM_H1_HW8_BS128", "host_s": fd_h.ct, "host_threads": os.cpu_count(),
+                          "gpu_s": dv_s, "note": "host: getFormatDataAXT (ispmv_build_axt, wall clock); "
+                                                 "gpu: ispmv_dev_build_axt on device CSR + x (CUDA events)"}
+        except Exception as e:
+            conversion = {"unavailable": str(e)[:120]}
 
     cpu = None
     if rank == 0 and ws == 1 and not a.no_cpu:
@@ -414,12 +457,148 @@ def main(argv=None):
             "clocks": clocks,
             "parity": check,
             "formats": formats,
+            "conversion": conversion,
         }
         print(json.dumps(out), flush=True)
     if ws > 1:
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
+
+
+def _event_time(fn, steps: int, warmup: int) -> float:
+    """Seconds per call of fn, CUDA events on the current stream."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / steps
+
+
+def main_spmm(a, rank, ws, W):
+    """Y = A X on the power-law generator at n = 1,000,000 (seed 3), X n x k
+    row-major U[-1, 1], k in {8, 16, 32}, FP64 and FP32 values; the plan
+    (format, kernel, RHS block) is the autotuner's choice for the matrix."""
+    import torch
+    torch.cuda.set_device(0)
+    from int_spmv_b200 import _lib, autotune
+    from int_spmv_b200 import formats as F
+    from oracle import Oracle
+    wl = make_workload("powerlaw1m")
+    csr = F.CSR(wl["row"], wl["col"], wl["val"])
+    n, nnz = csr.n, csr.nnz
+    orc = Oracle()
+    res, launches = {}, 0
+    for val in ("f64", "f32"):
+        for k in (8, 16, 32):
+            plan, choice = autotune.best_plan(csr, wl["x"], val=val, k=k, use_cache=False)
+            X = torch.from_numpy(np.random.default_rng(3).uniform(-1, 1, (n, k))).cuda()
+            Y = torch.empty_like(X)
+            l0 = _lib.launch_count()
+            plan.spmm(X, Y)
+            per = _lib.launch_count() - l0
+            t = _event_time(lambda: plan.spmm(X, Y), a.steps, W)
+            launches += per * a.steps
+            Yh, Xh = Y.cpu().numpy(), X.cpu().numpy()
+            err = 0.0
+            for j in (0, k // 2, k - 1):
+                xj = np.ascontiguousarray(Xh[:, j])
+                ref, ab = orc.cf_csr(wl["row"], wl["col"], wl["val"], xj), orc.abs_csr(wl["row"], wl["col"], wl["val"], xj)
+                err = max(err, float(np.max(np.abs(Yh[:, j] - ref) / np.maximum(ab, 1e-300))))
+            bval = 8 if val == "f64" else 4
+            B = nnz * (bval + 4) + n * k * 16 + 4 * (n + 1)
+            res[f"{val}/k{k}"] = {"ms": t * 1e3, "gflops": 2 * nnz * k / t / 1e9, "gbs": B / t / 1e9,
+                                  "format": choice["format"], "kwargs": choice["kwargs"],
+                                  "max_componentwise_err": err, "rhs_columns_checked": 3}
+            del plan
+    best = res["f64/k32"]
+    out = {"metric": "SpMM GFLOP/s (2*nnz*k)", "value": best["gflops"], "unit": "GFLOP/s", "n_gpus": 1,
+           "steps": a.steps, "warmup": W, "ms_per_step": best["ms"], "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic: power-law n=1,000,000 seed 3, X~U[-1,1]",
+           "config": {"workload": "spmm_powerlaw_n1M_seed3", "n": n, "nnz": nnz, "k": [8, 16, 32],
+                      "choice": "autotuned per (value form, k)"},
+           "gpu_launches": launches, "results": res}
+    print(json.dumps(out), flush=True)
+
+
+def main_batch(a, rank, ws, W):
+    """Many uneven FEM-like banded matrices (n log-uniform in [1e3, nmax],
+    rows of 7-81 entries within +/-3*rl of the diagonal; seed 4), each with
+    its own x: one block-diagonal plan in one CUDA-graph launch (the
+    lane-interleaved kernel, and the persistent work-queue kernel), against
+    one plan per matrix launched one after the other."""
+    import torch
+    torch.cuda.set_device(0)
+    from int_spmv_b200 import _lib
+    from int_spmv_b200 import batch as BT
+    from int_spmv_b200 import device as D
+    from int_spmv_b200 import formats as F
+    from int_spmv_b200 import matrices as M
+    from oracle import Oracle
+    t0 = time.time()
+    mats = M.fem_batch_c(count=a.batch_count, seed=4, n_lo=1e3, n_hi=a.batch_nmax)
+    big, off = BT.blockdiag(mats)
+    n, nnz = big.n, big.nnz
+    x = M.uniform_x(n, 4)
+    xt = torch.from_numpy(x).cuda()
+    res = {}
+    y = torch.empty(n, dtype=torch.float64, device="cuda")
+    for name, kw in (("graph_wide", dict(kernel="wide")), ("graph_queue", dict(kernel="ldg", variant=16))):
+        plan = D.Plan(big, None, val=a.val, **kw)
+        l0 = _lib.launch_count()
+        plan.spmv_graph(xt, y)
+        torch.cuda.synchronize()
+        t = _event_time(lambda: plan.spmv_graph(xt, y), a.steps, W)
+        res[name] = {"ms": t * 1e3, "gflops": 2 * nnz / t / 1e9, "gbs": plan.info["alg_bytes"] / t / 1e9,
+                     "kernel": plan.kernel_name(), "graph_launches_per_step": 1,
+                     "kernels_per_step": _lib.launch_count() - l0}
+        yb = y.cpu().numpy()
+        del plan
+    del big
+    # one plan per matrix, launched one after the other (2 launches each)
+    plans, ys, xs = [], [], []
+    for m, (row, col, val) in enumerate(mats):
+        csr = F.CSR(row, col, val)
+        plans.append(D.Plan(csr, None, kernel="wide", val=a.val))
+        xs.append(xt[int(off[m]):int(off[m + 1])])
+        ys.append(y[int(off[m]):int(off[m + 1])])
+
+    def each():
+        for p_, x_, y_ in zip(plans, xs, ys):
+            p_.spmv(x_, y_)
+    l0 = _lib.launch_count()
+    each()
+    per = _lib.launch_count() - l0
+    t = _event_time(each, max(3, a.steps // 4), W)
+    res["separate"] = {"ms": t * 1e3, "gflops": 2 * nnz / t / 1e9, "launches_per_step": per}
+    ys_sep = y.cpu().numpy()
+    # parity: every matrix of a sample against the oracle, and the batched y
+    orc, err = Oracle(), 0.0
+    tol = 1e-12 if a.val == "f64" else 1e-6
+    for m in sorted(set(np.linspace(0, len(mats) - 1, 16).astype(int))):
+        row, col, val = mats[m]
+        a0, a1 = int(off[m]), int(off[m + 1])
+        ref, ab = orc.cf_csr(row, col, val, x[a0:a1]), orc.abs_csr(row, col, val, x[a0:a1])
+        for yy in (yb, ys_sep):
+            err = max(err, float(np.max(np.abs(yy[a0:a1] - ref) / np.maximum(ab, 1e-300))))
+    out = {"metric": "batched SpMV GFLOP/s (2*sum nnz)", "value": res["graph_wide"]["gflops"], "unit": "GFLOP/s",
+           "n_gpus": 1, "steps": a.steps, "warmup": W, "ms_per_step": res["graph_wide"]["ms"],
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64" if a.val == "f64" else "f32-mul/f64-acc",
+           "data": f"synthetic: {a.batch_count} banded FEM-like matrices, n log-uniform in [1e3, {a.batch_nmax:g}], "
+                   "rl U[7,81] within +/-3 rl, seed 4 (int_spmv_b200/matrices.py fem_batch_c)",
+           "config": {"workload": f"fem_batch_{a.batch_count}_nmax{a.batch_nmax:g}", "matrices": len(mats),
+                      "n": n, "nnz": nnz, "value_kind": a.val},
+           "speedup_graph_vs_separate": res["separate"]["ms"] / res["graph_wide"]["ms"],
+           "parity": {"max_componentwise": err, "bound": tol, "pass": err <= tol, "matrices_checked": 16},
+           "results": res, "setup_s": time.time() - t0}
+    print(json.dumps(out), flush=True)
 
 
 def main_reference(a, rank, ws, W):

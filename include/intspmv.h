@@ -250,6 +250,21 @@ void int_axt_com_h1(const UIN ompNT, const UIN bn, const UIN bs, const UIN log, 
                     const UIN tn, const UIN lenAX, const UIN lenRWP, const FPT *ax,
                     const UIN *rwp, FPT *y);                                    /* M:1517 */
 
+/* Format conversion on the GPU (no reference counterpart: the reference
+ * converts on the host, getFormatDataAXT M:1275-1381).  Builds the same
+ * con/ax/sec arrays as getFormatDataAXT, bit for bit, from a CSR matrix and
+ * x in DEVICE memory (d_row n+1, d_col/d_val nnz, d_x n).  The struct's
+ * con/ax/sec are device pointers, to be released with ispmv_dev_axt_free;
+ * fd->ct is the conversion's GPU time in seconds.  Synchronises `stream`.
+ * Feed the result to ispmv_dev_int_axt_noc_h1 / _noc / _com_h1. */
+int ispmv_dev_build_axt(UIN bs, UIN thw, UIN th, const char *mode, UIN n, UIN nnz, const UIN *d_row,
+                        const UIN *d_col, const FPT *d_val, const FPT *d_x, str_matAXT *m,
+                        str_formatData *fd, void *stream);
+int ispmv_dev_axt_free(str_matAXT *m);
+/* Copies a device-built AXT's con/ax/sec (lenCON/lenAX/lenSEC entries) into
+ * caller buffers, host or device (NULL skips one); synchronises `stream`. */
+int ispmv_dev_axt_export(const str_matAXT *m, UIN *con, FPT *ax, UIN *sec, void *stream);
+
 /* ---------------------------------------------------------------------------
  * Layer 3: plans - a format resident in HBM as value/column streams; every
  * call gathers a fresh x through L2.  No reference counterpart: the

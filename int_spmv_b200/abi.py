@@ -68,6 +68,11 @@ P_PLAN = C.POINTER(VP)
 
 # name: (restype, argtypes).  Every `extern "C"` function of include/intspmv.h.
 PROTOTYPES: dict[str, tuple] = {
+    # format conversion on the GPU
+    "ispmv_dev_build_axt": (C.c_int, [UIN, UIN, UIN, C.c_char_p, UIN, UIN, VP, VP, VP, VP,
+                                      C.POINTER(StrMatAXT), C.POINTER(StrFormatData), VP]),
+    "ispmv_dev_axt_free": (C.c_int, [C.POINTER(StrMatAXT)]),
+    "ispmv_dev_axt_export": (C.c_int, [C.POINTER(StrMatAXT), VP, VP, VP, VP]),
     # self-test of the bounded device wait
     "ispmv_selftest_bounded_wait": (C.c_int, [C.POINTER(C.c_double), C.c_void_p]),
     # host: statistics, files, builders

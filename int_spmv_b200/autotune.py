@@ -3,9 +3,10 @@
 For a matrix it times candidate plans on the current GPU and keeps the
 fastest.  The candidates vary:
 - the format: AXT compacted, AXT tileHeight 1, 4, 8 or 16, AXC, CSR, K1;
-- the kernel family: slot stream with plain loads or bulk-copy staging,
-  tile columns, or row-parallel;
-- the kernel variant: slots per lane (the vector width), prefetch depth,
+- the kernel family: lane-interleaved slot stream (stream_wide), slot stream
+  with plain loads or bulk-copy staging, tile columns, or row-parallel;
+- the kernel variant: slots per lane (the vector width: 8 or 16 for
+  stream_wide, 2 or 4 for stream_ldg), prefetch depth or bulk-copy stages,
   warps per SM (threads per tile) and shared-memory x bands;
 - the segment size;
 - for SpMM, the right-hand sides per pass (the RHS block).
@@ -31,6 +32,13 @@ from .formats import CSR
 
 # (format, plan keyword arguments)
 SPMV_CANDIDATES = [
+    ("COM128", dict(kernel="wide", variant=0)),   # 16 slots per lane
+    ("COM128", dict(kernel="wide", variant=4)),   # 8 slots per lane
+    ("COM128", dict(kernel="wide", variant=8)),   # 16 slots per lane, 8192-slot segments
+    ("COM128", dict(kernel="wide", variant=9)),   # 16 slots per lane, 2048-slot segments
+    ("COM128", dict(kernel="wide", variant=11)),  # bulk-copy staged, 16 slots per lane
+    ("COM128", dict(kernel="wide", variant=7)),   # 8 slots per lane, shared-memory x band
+    ("NOC1", dict(kernel="wide", variant=0)),
     ("COM128", dict(kernel="ldg", variant=0)),
     ("COM128", dict(kernel="ldg", variant=2)),
     ("COM128", dict(kernel="ldg", variant=12)),

@@ -198,3 +198,62 @@ class Plan:
         xp = x.data_ptr() if isinstance(x, torch.Tensor) else x.ctypes.data
         yp = y.data_ptr() if isinstance(y, torch.Tensor) else y.ctypes.data
         check(load().ispmv_plan_spmv_host(self._h, xp, yp, _stream(stream)), "ispmv_plan_spmv_host")
+
+
+# --- format conversion on the GPU ---
+
+class DeviceAXT:
+    """getFormatDataAXT (intSpmv_main.c:1275) run on the GPU
+    (ispmv_dev_build_axt): con, the x-baked ax and sec of the AXT format, bit
+    for bit the host builder's, built from CSR arrays and x already on the
+    device (u32 arrays as int32 tensors).  The arrays stay in device memory
+    (owned here); `fd` is the format data with the GPU conversion time."""
+
+    def __init__(self, row: torch.Tensor, col: torch.Tensor, val: torch.Tensor, x: torch.Tensor, bs: int = 128,
+                 thw: int = 8, th: int = 1, mode: str = "COM", stream=None):
+        lib = load()
+        n, nnz = row.numel() - 1, col.numel()
+        self.c, self.fd = abi.StrMatAXT(), abi.StrFormatData()
+        check(lib.ispmv_dev_build_axt(bs, thw, th, mode.encode(), n, nnz, _ptr(row), _ptr(col) if nnz else None,
+                                      _ptr(val) if nnz else None, _ptr(x), C.byref(self.c), C.byref(self.fd),
+                                      _stream(stream)), "ispmv_dev_build_axt")
+
+    def __del__(self):
+        c = getattr(self, "c", None)
+        if c is not None and c.ax:
+            try:
+                load().ispmv_dev_axt_free(C.byref(c))
+            except Exception:
+                pass
+
+    @property
+    def conversion_s(self) -> float:
+        return float(self.fd.ct)
+
+    def to_host(self, stream=None) -> dict:
+        """con, ax and sec copied to numpy arrays."""
+        con = np.zeros(self.c.lenCON, np.uint32)
+        ax = np.zeros(self.c.lenAX, np.float64)
+        sec = np.zeros(self.c.lenSEC, np.uint32)
+        check(load().ispmv_dev_axt_export(C.byref(self.c), con.ctypes.data or None, ax.ctypes.data or None,
+                                          sec.ctypes.data or None, _stream(stream)), "ispmv_dev_axt_export")
+        return dict(con=con, ax=ax, sec=sec)
+
+    def spmv(self, y: torch.Tensor, stream=None) -> torch.Tensor:
+        """The reference kernel of this AXT (int_axt_noc_h1, int_axt_noc or
+        int_axt_com_h1) on the device arrays; like the reference it
+        accumulates into y (zero it first)."""
+        lib, c = load(), self.c
+        ax, sec = C.cast(c.ax, C.c_void_p), C.cast(c.sec, C.c_void_p)
+        mode = c.mode.decode()
+        if mode == "NOC" and c.tileH == 1:
+            check(lib.ispmv_dev_int_axt_noc_h1(c.tileN, ax, sec, _ptr(y), _stream(stream)), "ispmv_dev_int_axt_noc_h1")
+        elif mode == "NOC":
+            check(lib.ispmv_dev_int_axt_noc(c.tileN, c.tileH, ax, sec, _ptr(y), _stream(stream)),
+                  "ispmv_dev_int_axt_noc")
+        else:
+            bs = 1 << c.log
+            bn = (c.lenSEC + bs - 1) // bs  # blocks of bs slots (intSpmv_main.c:1517)
+            check(lib.ispmv_dev_int_axt_com_h1(bn, bs, c.log, c.tileHW, c.tileN, c.lenAX, c.lenSEC, ax, sec, _ptr(y),
+                                               _stream(stream)), "ispmv_dev_int_axt_com_h1")
+        return y
