@@ -56,6 +56,7 @@ struct ispmv_plan_s {
   sss::XWin xw{};         // x bands staged in shared memory (variants >= 8)
   double lo_frac = 0.0;   // fraction of slots carrying a lo-word
   size_t esc_batches = 0; // D16 batches kept as u32 columns
+  size_t d16_batch = 128;  // D16 slots per base column (128; 32*slots per lane for stream_wide)
   FPT *hx = nullptr, *hy = nullptr;  // device staging of ispmv_plan_spmv_host
   float *x32 = nullptr;              // FP32 copy of x (FP32-value stream_wide plans)
   unsigned long long *queue = nullptr;  // work-queue counter (variant ISPMV_VARIANT_QUEUE)
@@ -148,8 +149,8 @@ void finish_info(ispmv_plan_s *p, const char *name) {
   double bv = (double)vbytes(p), bi = 4.0;
   if (p->opts.val_kind == ISPMV_VAL_F32_LO16) bv = 4.0 + 2.0 * p->lo_frac;
   if (p->opts.col_kind == ISPMV_COL_D16 && p->slots_pad) {
-    const double batches = (double)(p->slots_pad / 128);
-    bi = 2.0 + (4.0 * batches + 128.0 * 4.0 * (double)p->esc_batches) / std::max(1.0, (double)p->nnz);
+    const double B = (double)p->d16_batch, batches = (double)(p->slots_pad / p->d16_batch);
+    bi = 2.0 + (4.0 * batches + B * 4.0 * (double)p->esc_batches) / std::max(1.0, (double)p->nnz);
   }
   i.alg_bytes = (double)p->nnz * (bv + bi) + (double)p->n * 16.0 + 4.0 * ((double)p->n + 1.0);
   snprintf(i.name, sizeof i.name, "%s", name);
@@ -318,8 +319,10 @@ int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v,
   bool xwv = p->opts.kernel == ISPMV_KERNEL_LDG && !narrow_kinds(p) && xw_variant(p->opts.variant, &xc);
   const bool wide = p->opts.kernel == ISPMV_KERNEL_WIDE;
   if (wide) {
-    if (narrow_kinds(p)) return fail(ISPMV_ERR_UNSUPPORTED, "stream_wide: FP64/FP32 values with u32 columns only");
     const WideCfg wc = wide_variant(p->opts.variant);
+    if (p->opts.val_kind == ISPMV_VAL_F32_LO16 || (p->opts.col_kind == ISPMV_COL_D16 && (wc.win || wc.tma || wc.buf)))
+      return fail(ISPMV_ERR_UNSUPPORTED,
+                  "stream_wide: FP64/FP32 values; 16-bit column deltas on the plain-load variants without x bands");
     xc = {wc.warps, wc.cap, wc.seg};
     xwv = wc.win;
   }
@@ -345,12 +348,41 @@ int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v,
       ci[wide::il_pos(q, spl, 4u)] = c[q];
     }
     TRY(upload_values(p, vi));
-    TRY(dev_upload(p, ci.data(), ci.size(), &p->col));
+    if (p->opts.col_kind == ISPMV_COL_U32) {
+      TRY(dev_upload(p, ci.data(), ci.size(), &p->col));
+    } else {
+      // per batch of 32*spl slots: base = the smallest column among nonzero
+      // values, deltas to it in 16 bits (lane-interleaved, 8 per vector), or
+      // the batch's interleaved u32 columns when the span is wider
+      const size_t BT = 32u * spl, nb = p->slots_pad / BT;
+      p->d16_batch = BT;
+      std::vector<UIN> cmeta(nb), esc;
+      std::vector<uint16_t> c16(p->slots_pad, 0);
+      for (size_t b = 0; b < nb; b++) {
+        UIN lo = 0xFFFFFFFFu, hi = 0;
+        for (size_t q = b * BT; q < b * BT + BT; q++)
+          if (v[q] != 0.0) { lo = std::min(lo, c[q]); hi = std::max(hi, c[q]); }
+        if (lo == 0xFFFFFFFFu) lo = hi = 0;
+        if (hi - lo <= 0xFFFFu && lo < sss::ESCAPE) {
+          cmeta[b] = lo;
+          for (size_t q = b * BT; q < b * BT + BT; q++)
+            c16[wide::il_pos(q, spl, 8u)] = v[q] != 0.0 ? (uint16_t)(c[q] - lo) : 0;
+        } else {
+          cmeta[b] = sss::ESCAPE | (UIN)p->esc_batches++;
+          esc.insert(esc.end(), ci.begin() + b * BT, ci.begin() + b * BT + BT);  // interleaved already
+        }
+      }
+      uint16_t *d16; UIN *dm, *de;
+      TRY(dev_upload(p, c16.data(), c16.size(), &d16));
+      TRY(dev_upload(p, cmeta.data(), cmeta.size(), &dm));
+      TRY(dev_upload(p, esc.data(), esc.size(), &de));
+      p->narrow.col16 = d16; p->narrow.cmeta = dm; p->narrow.esc = de;
+    }
   } else {
     TRY(upload_values(p, v));
     if (p->opts.col_kind == ISPMV_COL_U32) TRY(dev_upload(p, c.data(), c.size(), &p->col));
   }
-  if (p->opts.col_kind == ISPMV_COL_D16) {
+  if (p->opts.col_kind == ISPMV_COL_D16 && !wide) {
     // per 128-slot batch: base = the smallest column among nonzero values;
     // deltas to it in 16 bits, or the batch's u32 columns when the span is wider
     const size_t nb = p->slots_pad / 128;
@@ -418,7 +450,8 @@ int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v,
   TRY(empty_rows(p, csr));
   TRY(alloc_records(p));
   p->info.device_bytes = (uint64_t)p->slots_pad * vbytes(p) + p->slots_pad / 8 +
-                         (p->opts.col_kind == ISPMV_COL_D16 ? p->slots_pad * 2 + p->slots_pad / 32 + p->esc_batches * 512
+                         (p->opts.col_kind == ISPMV_COL_D16 ? p->slots_pad * 2 + p->slots_pad / p->d16_batch * 4 +
+                                                                 p->esc_batches * p->d16_batch * 4
                                                            : p->slots_pad * 4) +
                          (uint64_t)(p->lo_frac * (double)p->slots_pad * 2.0);
   return ISPMV_OK;
@@ -586,7 +619,7 @@ ISPMV_API int ispmv_plan_axt(const str_matCSR *csr, const str_matAXT *axt, const
     if (p->opts.kernel == ISPMV_KERNEL_AUTO) {
       // the lane-interleaved kernel where it takes the value/column forms;
       // 16 slots per lane for rows of 16 slots or more on average, else 8
-      if (narrow_kinds(p)) {
+      if (p->opts.val_kind == ISPMV_VAL_F32_LO16) {
         p->opts.kernel = ISPMV_KERNEL_LDG;
       } else {
         p->opts.kernel = ISPMV_KERNEL_WIDE;
@@ -669,7 +702,7 @@ int launch_staged_w(K kernel, size_t smem, size_t nseg, int ctas_per_sm, cudaStr
   return check_launch(what);
 }
 
-template <typename VT, int SPL, int NW, int MINB, bool BUF>
+template <typename VT, int SPL, int NW, int MINB, bool BUF, bool D16 = false>
 int launch_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, const char *name) {
   if constexpr (sizeof(VT) == 4 && NW == 0) {
     // FP32 values: gather from an FP32 copy of x (the value the FP32 multiply uses)
@@ -678,21 +711,21 @@ int launch_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, cons
     if ((reinterpret_cast<uintptr_t>(x) & 15u) == 0) wide::x_to_f32<true><<<gc, 256, 0, s>>>(p->n, x, p->x32);
     else wide::x_to_f32<false><<<gc, 256, 0, s>>>(p->n, x, p->x32);
     TRY(check_launch("x_to_f32"));
-    auto *k = wide::stream_wide<VT, float, SPL, NW, WIDE_WARPS, MINB, BUF>;
+    auto *k = wide::stream_wide<VT, float, SPL, NW, WIDE_WARPS, MINB, BUF, D16>;
     const size_t smem = (BUF ? (size_t)WIDE_WARPS * 32 * SPL : 0) * sizeof(double);
     if (smem) ISPMV_TRY(cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k<<<(unsigned)((p->nseg + WIDE_WARPS - 1) / WIDE_WARPS), WIDE_WARPS * 32, smem, s>>>(
         p->slots, p->slots_pad, p->seg_slots, p->nseg, static_cast<const VT *>(p->val), p->col, p->heads, p->segh,
-        p->xw, p->x32, o);
+        p->xw, p->x32, o, p->narrow);
     return check_launch(name);
   }
-  auto *k = wide::stream_wide<VT, double, SPL, NW, WIDE_WARPS, MINB, BUF>;
+  auto *k = wide::stream_wide<VT, double, SPL, NW, WIDE_WARPS, MINB, BUF, D16>;
   const size_t smem =
       ((NW ? (size_t)p->xw.cap : 0) + (BUF ? (size_t)WIDE_WARPS * 32 * SPL : 0)) * sizeof(double);
   if (smem) ISPMV_TRY(cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const unsigned g = (unsigned)((p->nseg + WIDE_WARPS - 1) / WIDE_WARPS);
   k<<<g, WIDE_WARPS * 32, smem, s>>>(p->slots, p->slots_pad, p->seg_slots, p->nseg, static_cast<const VT *>(p->val),
-                                      p->col, p->heads, p->segh, p->xw, x, o);
+                                      p->col, p->heads, p->segh, p->xw, x, o, p->narrow);
   return check_launch(name);
 }
 
@@ -734,6 +767,11 @@ int run_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
     }
   }
   const int nw = wc.win ? std::min(std::max(p->xw.nwin, 0), 3) : 0;
+  if (p->opts.col_kind == ISPMV_COL_D16) {  // plain loads, no bands, direct row writes (setup checks)
+    if (wc.spl == 8) return launch_wide<VT, 8, 0, 4, false, true>(p, x, o, s, "stream_wide<8,w0,b4,buf0,d16>");
+    if (wc.minb == 2) return launch_wide<VT, 16, 0, 2, false, true>(p, x, o, s, "stream_wide<16,w0,b2,buf0,d16>");
+    return launch_wide<VT, 16, 0, 3, false, true>(p, x, o, s, "stream_wide<16,w0,b3,buf0,d16>");
+  }
   if (wc.spl == 8) {
     if (wc.buf) { ISPMV_WIDE_NW(8, 4, 1) }
     ISPMV_WIDE_NW(8, 4, 0)

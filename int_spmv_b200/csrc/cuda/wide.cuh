@@ -83,6 +83,22 @@ struct Cols {
   }
 };
 
+// SPL 16-bit column deltas of one lane (lane-interleaved, 8 per 16-byte load).
+template <int SPL>
+struct Deltas {
+  uint4 q[SPL / 8];
+  __device__ __forceinline__ void get(const uint16_t *d, size_t b, unsigned lane) {
+#pragma unroll
+    for (int i = 0; i < SPL / 8; i++) q[i] = ld_stream(reinterpret_cast<const uint4 *>(d + b + 256 * i + 8 * lane));
+  }
+  __device__ __forceinline__ UIN operator[](int k) const {
+    const uint4 &t = q[k >> 3];
+    const int w = (k & 7) >> 1;
+    const UIN word = w == 0 ? t.x : w == 1 ? t.y : w == 2 ? t.z : t.w;
+    return (k & 1) ? word >> 16 : word & 0xFFFFu;
+  }
+};
+
 // acc + v*x in the plan's value form: FP64 values fused multiply-add; FP32
 // values multiplied in FP32 (x rounded to FP32, or gathered from the plan's
 // FP32 copy of x, the same value) and added in FP64.
@@ -264,11 +280,15 @@ __device__ __forceinline__ void batch(const VT (&v)[SPL], const XT (&xv)[SPL], u
 // registers.  NW = number of shared-memory x bands (0: every gather through
 // L1/L2).  Dynamic shared memory: xw.cap doubles of bands (NW > 0), then
 // (BUF) WARPS row buffers of 32*SPL doubles.
-template <typename VT, typename XT, int SPL, int NW, int WARPS, int MINB, bool BUF>
+// D16: columns as 16-bit deltas to a per-batch base column (nw.cmeta, one
+// per batch of 32*SPL slots), lane-interleaved like the values; a batch whose
+// columns span more than 16 bits keeps its u32 columns in nw.esc (cmeta =
+// ESCAPE | its index there).
+template <typename VT, typename XT, int SPL, int NW, int WARPS, int MINB, bool BUF, bool D16 = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
     stream_wide(size_t nslots, size_t nslots_pad, size_t seg_slots, size_t nseg, const VT *__restrict__ val,
                 const UIN *__restrict__ col, const UIN *__restrict__ heads, const UIN *__restrict__ segh,
-                sss::XWin xw, const XT *__restrict__ x, seg::Out o) {
+                sss::XWin xw, const XT *__restrict__ x, seg::Out o, sss::Narrow nw = {}) {
   static_assert(NW == 0 || sizeof(XT) == 8, "shared-memory x bands hold FP64 x");
   constexpr int BT = 32 * SPL;
   constexpr unsigned MASK = SPL == 32 ? 0xffffffffu : (1u << SPL) - 1u;
@@ -328,8 +348,26 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
     const size_t b = s0 + (size_t)j * BT;
     Vals<VT, SPL> v;
     v.get(val, b, lane);
-    Cols<SPL> c;
-    c.get(col, b, lane);
+    UIN c[SPL];
+    if constexpr (D16) {
+      const UIN m = __ldg(nw.cmeta + b / BT);  // the same word for the whole warp
+      if (m & sss::ESCAPE) {
+        Cols<SPL> e;
+        e.get(nw.esc + (size_t)(m & ~sss::ESCAPE) * BT, 0, lane);
+#pragma unroll
+        for (int k = 0; k < SPL; k++) c[k] = e[k];
+      } else {
+        Deltas<SPL> d;
+        d.get(nw.col16, b, lane);
+#pragma unroll
+        for (int k = 0; k < SPL; k++) c[k] = m + d[k];
+      }
+    } else {
+      Cols<SPL> e;
+      e.get(col, b, lane);
+#pragma unroll
+      for (int k = 0; k < SPL; k++) c[k] = e[k];
+    }
     const unsigned bits = (__ldg(heads + (b >> 5) + ((SPL * lane) >> 5)) >> ((SPL * lane) & 31u)) & MASK;
     XT xv[SPL];
 #pragma unroll

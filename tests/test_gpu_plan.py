@@ -145,15 +145,38 @@ def test_wide_rejects_other_forms(env):
     g = load_golden("random257_empty")
     csr = F.CSR(g["row"], g["col"], g["val"])
     with pytest.raises(IntSpmvError):
-        make_plan(F, D, csr, g["x"], "COM128", col="d16", kernel="wide")
+        make_plan(F, D, csr, g["x"], "COM128", col="d16", kernel="wide", variant=2)  # x bands: u32 columns only
+    with pytest.raises(IntSpmvError):
+        make_plan(F, D, csr, g["x"], "COM128", col="d16", kernel="wide", variant=1)  # row buffer: u32 columns only
     with pytest.raises(IntSpmvError):
         make_plan(F, D, csr, g["x"], "COM128", val="f32lo", kernel="wide")
+
+
+WIDE_D16 = [0, 4, 8, 9, 14, 15]
+
+
+@pytest.mark.parametrize("fmt", ["COM128", "NOC1", "CSR"])
+@pytest.mark.parametrize("variant", WIDE_D16)
+@pytest.mark.parametrize("val_kind", ["f64", "f32"])
+def test_wide_d16(env, fmt, variant, val_kind):
+    """16-bit column deltas per batch of the lane-interleaved kernel: banded
+    matrices (deltas), random ones (batches escape to u32 columns) and long
+    rows spanning segments."""
+    from int_spmv_b200 import matrices as M
+    mats = [M.fem_banded(20011, np.random.default_rng(5), 3, 30), M.stencil27(22, seed=2),
+            M.random_csr(7001, 12, rl_max=90, empty_frac=0.1), M.random_csr(3001, 9, rl_max=700, empty_frac=0.2)]
+    for i, (row, col, val) in enumerate(mats):
+        x = M.uniform_x(len(row) - 1, 30 + i)
+        for beta in (0, 1):
+            p, _ = check_plan(env, row, col, val, x, fmt, val_kind, beta, kernel="wide", variant=variant, col="d16")
+            assert p.info["kernel"] == 4 and p.info["col_kind"] == 1 and p.kernel_name().endswith("d16>")
 
 
 @pytest.mark.parametrize("fmt", ["COM128", "NOC1"])
 def test_auto_picks_wide(env, fmt):
     """AXT COM and tileH=1 plans default to the lane-interleaved kernel: 16
-    slots per lane for long rows, 8 for short; narrow forms keep stream_ldg."""
+    slots per lane for long rows, 8 for short, u32 or 16-bit columns; the
+    BF16 lo-word form keeps stream_ldg."""
     torch, D, F, orc = env
     from int_spmv_b200 import matrices as M
     for rl_max, spl in ((8, "<8,"), (60, "<16,")):
@@ -162,6 +185,8 @@ def test_auto_picks_wide(env, fmt):
         p, _ = check_plan(env, row, col, val, x, fmt)
         assert p.info["kernel"] == 4 and p.kernel_name().startswith("stream_wide" + spl)
         p, _ = check_plan(env, row, col, val, x, fmt, col="d16")
+        assert p.info["kernel"] == 4 and p.kernel_name().endswith("d16>")
+        p, _ = check_plan(env, row, col, val, x, fmt, val_kind="f32lo")
         assert p.info["kernel"] == 1
 
 
