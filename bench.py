@@ -405,10 +405,14 @@ def main(argv=None):
     if not a.no_formats:
         try:
             fd_h, _ = F.getFormatDataAXT(0, 128, 8, 1, "COM", csr, wl["x"])
-            dv = D.DeviceAXT(D.to_device(wl["row"]), D.to_device(wl["col"]), D.to_device(wl["val"]), x,
-                             bs=128, th=1, mode="COM")
-            dv_s = dv.conversion_s
-            del dv
+            drow, dcol, dval = D.to_device(wl["row"]), D.to_device(wl["col"]), D.to_device(wl["val"])
+            dv_s = []
+            for _ in range(2):  # the first call also loads the builder's kernels
+                dv = D.DeviceAXT(drow, dcol, dval, x, bs=128, th=1, mode="COM")
+                dv_s.append(dv.conversion_s)
+                del dv
+            dv_s = dv_s[-1]
+            del drow, dcol, dval
             conversion = {"format": "AXT_COM_H1_HW8_BS128", "host_s": fd_h.ct, "host_threads": os.cpu_count(),
                           "gpu_s": dv_s, "note": "host: getFormatDataAXT (ispmv_build_axt, wall clock); "
                                                  "gpu: ispmv_dev_build_axt on device CSR + x (CUDA events)"}

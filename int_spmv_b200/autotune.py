@@ -38,6 +38,7 @@ SPMV_CANDIDATES = [
     ("COM128", dict(kernel="wide", variant=9)),   # 16 slots per lane, 2048-slot segments
     ("COM128", dict(kernel="wide", variant=11)),  # bulk-copy staged, 16 slots per lane
     ("COM128", dict(kernel="wide", variant=7)),   # 8 slots per lane, shared-memory x band
+    ("COM128", dict(kernel="wide", variant=16)),  # 8 slots per lane, x gathered through the texture pipe
     ("NOC1", dict(kernel="wide", variant=0)),
     ("COM128", dict(kernel="ldg", variant=0)),
     ("COM128", dict(kernel="ldg", variant=2)),

@@ -59,6 +59,9 @@ struct ispmv_plan_s {
   size_t d16_batch = 128;  // D16 slots per base column (128; 32*slots per lane for stream_wide)
   FPT *hx = nullptr, *hy = nullptr;  // device staging of ispmv_plan_spmv_host
   float *x32 = nullptr;              // FP32 copy of x (FP32-value stream_wide plans)
+  cudaTextureObject_t xtex = 0;      // linear texture over x (stream_wide texture-gather variants)
+  const void *xtex_src = nullptr;    // the buffer it covers
+  size_t xtex_bytes = 0;
   unsigned long long *queue = nullptr;  // work-queue counter (variant ISPMV_VARIANT_QUEUE)
   cudaStream_t cap_stream = nullptr;    // private stream for graph capture
   cudaGraph_t graph = nullptr;
@@ -232,7 +235,9 @@ bool xw_variant(int v, XwCfg *c) {
 // registers are sized for (plain loads); rows through a per-warp buffer
 // (coalesced y stores) or written by the lane that ends them; and for the
 // staged form (tma) the stages per warp and warps per CTA.
-struct WideCfg { int spl; bool win; UIN cap; size_t seg; int minb; bool buf; bool tma; int stages; int warps; };
+struct WideCfg {
+  int spl; bool win; UIN cap; size_t seg; int minb; bool buf; bool tma; int stages; int warps; bool tex = false;
+};
 constexpr int WIDE_WARPS = 8;
 WideCfg wide_variant(int v) {
   switch (v) {
@@ -251,6 +256,8 @@ WideCfg wide_variant(int v) {
     case 13: return {8, false, 0, 4096, 0, false, true, 4, 4};
     case 14: return {16, false, 0, 4096, 2, false, false, 0, 8};
     case 15: return {16, false, 0, 8192, 2, false, false, 0, 8};
+    case 16: return {8, false, 0, 2048, 4, false, false, 0, 8, true};   // texture gathers
+    case 17: return {16, false, 0, 4096, 3, false, false, 0, 8, true};
     default: return {16, false, 0, 4096, 3, false, false, 0, 8};
   }
 }
@@ -470,6 +477,7 @@ ISPMV_API void ispmv_plan_opts_default(ispmv_plan_opts *o) {
 ISPMV_API int ispmv_plan_destroy(ispmv_plan p) {
   if (!p) return ISPMV_OK;
   for (cudaEvent_t e : p->tev) cudaEventDestroy(e);
+  if (p->xtex) cudaDestroyTextureObject(p->xtex);
   if (p->graph_exec) cudaGraphExecDestroy(p->graph_exec);
   if (p->graph) cudaGraphDestroy(p->graph);
   if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
@@ -617,13 +625,19 @@ ISPMV_API int ispmv_plan_axt(const str_matCSR *csr, const str_matAXT *axt, const
     std::vector<size_t> start(p->n);
     for (UIN r = 0; r < p->n; r++) start[r] = (size_t)(axt->con[r] / 16) * 8 + axt->con[r] % 16;
     if (p->opts.kernel == ISPMV_KERNEL_AUTO) {
-      // the lane-interleaved kernel where it takes the value/column forms;
-      // 16 slots per lane for rows of 16 slots or more on average, else 8
+      // the lane-interleaved kernel where it takes the value/column forms:
+      // 8 slots per lane for rows of fewer than 16 slots on average; else 16,
+      // bulk-copy staged for FP64 values with u32 columns (measured fastest
+      // there), plain loads for the FP32 and 16-bit-delta forms
       if (p->opts.val_kind == ISPMV_VAL_F32_LO16) {
         p->opts.kernel = ISPMV_KERNEL_LDG;
       } else {
         p->opts.kernel = ISPMV_KERNEL_WIDE;
-        if (p->opts.variant == 0) p->opts.variant = (double)p->slots >= 16.0 * (double)p->n ? 0 : 4;
+        if (p->opts.variant == 0) {
+          const bool long_rows = (double)p->slots >= 16.0 * (double)p->n;
+          const bool plain = p->opts.val_kind == ISPMV_VAL_F64 && p->opts.col_kind == ISPMV_COL_U32;
+          p->opts.variant = !long_rows ? 4 : plain ? 11 : 0;
+        }
       }
     }
     st = setup_stream(p, csr, v, c, start);
@@ -702,7 +716,42 @@ int launch_staged_w(K kernel, size_t smem, size_t nseg, int ctas_per_sm, cudaStr
   return check_launch(what);
 }
 
-template <typename VT, int SPL, int NW, int MINB, bool BUF, bool D16 = false>
+// A linear texture over `src` (bytes long, FP64 read as int2 or FP32),
+// cached on the plan for the same buffer; 0 when the buffer does not meet
+// the texture alignment or size limits (the caller then gathers with loads).
+// Not inside graph capture: a later product with another x replaces the
+// texture, which a captured graph would still name.
+cudaTextureObject_t x_texture(ispmv_plan_s *p, const void *src, size_t bytes, bool f32) {
+  if (p->capturing) return 0;
+  if (p->xtex && p->xtex_src == src && p->xtex_bytes == bytes) return p->xtex;
+  if (p->xtex) cudaDestroyTextureObject(p->xtex);
+  p->xtex = 0;
+  p->xtex_src = nullptr;
+  int dev = 0, align = 0, maxw = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&align, cudaDevAttrTextureAlignment, dev) ||
+      cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxTexture1DLinearWidth, dev))
+    return 0;
+  const size_t elems = bytes / (f32 ? 4 : 8);
+  if (align <= 0 || reinterpret_cast<uintptr_t>(src) % (uintptr_t)align || elems > (size_t)maxw || elems >= (1u << 31))
+    return 0;
+  cudaResourceDesc rd{};
+  rd.resType = cudaResourceTypeLinear;
+  rd.res.linear.devPtr = const_cast<void *>(src);
+  rd.res.linear.desc = f32 ? cudaCreateChannelDesc<float>() : cudaCreateChannelDesc<int2>();
+  rd.res.linear.sizeInBytes = bytes;
+  cudaTextureDesc td{};
+  td.readMode = cudaReadModeElementType;
+  if (cudaCreateTextureObject(&p->xtex, &rd, &td, nullptr) != cudaSuccess) {
+    cudaGetLastError();
+    p->xtex = 0;
+    return 0;
+  }
+  p->xtex_src = src;
+  p->xtex_bytes = bytes;
+  return p->xtex;
+}
+
+template <typename VT, int SPL, int NW, int MINB, bool BUF, bool D16 = false, bool TEX = false>
 int launch_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, const char *name) {
   if constexpr (sizeof(VT) == 4 && NW == 0) {
     // FP32 values: gather from an FP32 copy of x (the value the FP32 multiply uses)
@@ -711,21 +760,27 @@ int launch_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, cons
     if ((reinterpret_cast<uintptr_t>(x) & 15u) == 0) wide::x_to_f32<true><<<gc, 256, 0, s>>>(p->n, x, p->x32);
     else wide::x_to_f32<false><<<gc, 256, 0, s>>>(p->n, x, p->x32);
     TRY(check_launch("x_to_f32"));
-    auto *k = wide::stream_wide<VT, float, SPL, NW, WIDE_WARPS, MINB, BUF, D16>;
+    const cudaTextureObject_t tx = TEX ? x_texture(p, p->x32, (size_t)p->n * 4, true) : 0;
+    if (TEX && !tx)
+      return launch_wide<VT, SPL, NW, MINB, BUF, D16, false>(p, x, o, s, "stream_wide<tex: x gathered with loads>");
+    auto *k = wide::stream_wide<VT, float, SPL, NW, WIDE_WARPS, MINB, BUF, D16, TEX>;
     const size_t smem = (BUF ? (size_t)WIDE_WARPS * 32 * SPL : 0) * sizeof(double);
     if (smem) ISPMV_TRY(cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k<<<(unsigned)((p->nseg + WIDE_WARPS - 1) / WIDE_WARPS), WIDE_WARPS * 32, smem, s>>>(
         p->slots, p->slots_pad, p->seg_slots, p->nseg, static_cast<const VT *>(p->val), p->col, p->heads, p->segh,
-        p->xw, p->x32, o, p->narrow);
+        p->xw, p->x32, o, p->narrow, tx);
     return check_launch(name);
   }
-  auto *k = wide::stream_wide<VT, double, SPL, NW, WIDE_WARPS, MINB, BUF, D16>;
+  const cudaTextureObject_t tx = TEX ? x_texture(p, x, (size_t)p->n * 8, false) : 0;
+  if (TEX && !tx)
+    return launch_wide<VT, SPL, NW, MINB, BUF, D16, false>(p, x, o, s, "stream_wide<tex: x gathered with loads>");
+  auto *k = wide::stream_wide<VT, double, SPL, NW, WIDE_WARPS, MINB, BUF, D16, TEX>;
   const size_t smem =
       ((NW ? (size_t)p->xw.cap : 0) + (BUF ? (size_t)WIDE_WARPS * 32 * SPL : 0)) * sizeof(double);
   if (smem) ISPMV_TRY(cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   const unsigned g = (unsigned)((p->nseg + WIDE_WARPS - 1) / WIDE_WARPS);
   k<<<g, WIDE_WARPS * 32, smem, s>>>(p->slots, p->slots_pad, p->seg_slots, p->nseg, static_cast<const VT *>(p->val),
-                                      p->col, p->heads, p->segh, p->xw, x, o, p->narrow);
+                                      p->col, p->heads, p->segh, p->xw, x, o, p->narrow, tx);
   return check_launch(name);
 }
 
@@ -767,6 +822,14 @@ int run_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
     }
   }
   const int nw = wc.win ? std::min(std::max(p->xw.nwin, 0), 3) : 0;
+  if (wc.tex) {  // texture gathers (loads where x does not fit a texture)
+    const bool d = p->opts.col_kind == ISPMV_COL_D16;
+    if (wc.spl == 8)
+      return d ? launch_wide<VT, 8, 0, 4, false, true, true>(p, x, o, s, "stream_wide<8,w0,b4,buf0,d16,tex>")
+               : launch_wide<VT, 8, 0, 4, false, false, true>(p, x, o, s, "stream_wide<8,w0,b4,buf0,tex>");
+    return d ? launch_wide<VT, 16, 0, 3, false, true, true>(p, x, o, s, "stream_wide<16,w0,b3,buf0,d16,tex>")
+             : launch_wide<VT, 16, 0, 3, false, false, true>(p, x, o, s, "stream_wide<16,w0,b3,buf0,tex>");
+  }
   if (p->opts.col_kind == ISPMV_COL_D16) {  // plain loads, no bands, direct row writes (setup checks)
     if (wc.spl == 8) return launch_wide<VT, 8, 0, 4, false, true>(p, x, o, s, "stream_wide<8,w0,b4,buf0,d16>");
     if (wc.minb == 2) return launch_wide<VT, 16, 0, 2, false, true>(p, x, o, s, "stream_wide<16,w0,b2,buf0,d16>");

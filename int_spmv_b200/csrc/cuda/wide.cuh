@@ -14,17 +14,19 @@
 //     owns the SPL consecutive slots b + SPL*l + k, and element (l, k) sits at
 //     b + (k / V)*32*V + l*V + k % V with V = 16 / sizeof(element), so every
 //     vector load of the warp is 512 contiguous bytes;
-//   - gathers a column that falls in one of the plan's diagonal bands from
-//     shared memory (a few bank wavefronts per warp instead of up to 32 L1
-//     wavefronts), and any other column from x through L1/L2.  Which path
-//     serves a column does not change the result.
+//   - gathers x through L1/L2 with plain loads; variants gather a column
+//     that falls in one of the plan's diagonal bands from shared memory, or
+//     every column through the texture pipe.  Which path serves a column
+//     does not change the result;
+//   - FP32-value plans gather an FP32 copy of x made once per product, and
+//     columns may be 16-bit deltas to a per-batch base (D16).
 // The row reduction is the slot stream's: rows are contiguous runs of
 // slots, row starts are bits of `heads` (slot order), a warp owns a segment
 // of slots and leaves two (row, partial) records per segment for
-// seg::fixup.  The rows a batch completes pass through a per-warp buffer in
-// shared memory and reach y as coalesced stores.  Every row is written
-// exactly once, without atomics, and the summation order is fixed, so
-// results are bitwise repeatable.
+// seg::fixup.  A row is written by the lane that ends it, or (BUF) through
+// a per-warp buffer in shared memory as coalesced stores.  Every row is
+// written exactly once, without atomics, and the summation order is fixed,
+// so results are bitwise repeatable.
 //
 // stream_wide_tma is the same reduction fed by 1D bulk copies
 // (cp.async.bulk, no multicast) into a per-warp ring of stages in shared
@@ -284,12 +286,17 @@ __device__ __forceinline__ void batch(const VT (&v)[SPL], const XT (&xv)[SPL], u
 // per batch of 32*SPL slots), lane-interleaved like the values; a batch whose
 // columns span more than 16 bits keeps its u32 columns in nw.esc (cmeta =
 // ESCAPE | its index there).
-template <typename VT, typename XT, int SPL, int NW, int WARPS, int MINB, bool BUF, bool D16 = false>
+// TEX: x is gathered with texture fetches (tex1Dfetch on `xtex`, a linear
+// texture over x) instead of global loads: the texture pipe of L1TEX serves
+// the gathers while the load/store pipe streams values and columns.
+template <typename VT, typename XT, int SPL, int NW, int WARPS, int MINB, bool BUF, bool D16 = false, bool TEX = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
     stream_wide(size_t nslots, size_t nslots_pad, size_t seg_slots, size_t nseg, const VT *__restrict__ val,
                 const UIN *__restrict__ col, const UIN *__restrict__ heads, const UIN *__restrict__ segh,
-                sss::XWin xw, const XT *__restrict__ x, seg::Out o, sss::Narrow nw = {}) {
+                sss::XWin xw, const XT *__restrict__ x, seg::Out o, sss::Narrow nw = {},
+                cudaTextureObject_t xtex = 0) {
   static_assert(NW == 0 || sizeof(XT) == 8, "shared-memory x bands hold FP64 x");
+  static_assert(!(TEX && NW > 0), "texture gathers replace the shared-memory bands");
   constexpr int BT = 32 * SPL;
   constexpr unsigned MASK = SPL == 32 ? 0xffffffffu : (1u << SPL) - 1u;
   extern __shared__ __align__(16) double sx[];
@@ -372,8 +379,18 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
     XT xv[SPL];
 #pragma unroll
     for (int k = 0; k < SPL; k++) {
-      if constexpr (NW > 0) xv[k] = gather<NW>(w, sxa, x, c[k]);
-      else xv[k] = __ldg(x + c[k]);
+      if constexpr (NW > 0) {
+        xv[k] = gather<NW>(w, sxa, x, c[k]);
+      } else if constexpr (TEX) {
+        if constexpr (sizeof(XT) == 8) {
+          const int2 t = tex1Dfetch<int2>(xtex, (int)c[k]);
+          xv[k] = __hiloint2double(t.y, t.x);
+        } else {
+          xv[k] = tex1Dfetch<float>(xtex, (int)c[k]);
+        }
+      } else {
+        xv[k] = __ldg(x + c[k]);
+      }
     }
     VT vv[SPL];
 #pragma unroll

@@ -21,7 +21,7 @@ COMBOS = [("CSR", "rows"), ("CSR", "ldg"), ("CSR", "tma"), ("AXC", "rows"), ("AX
           ("COM128", "ldg"), ("COM128", "tma"), ("COM256", "ldg"), ("COM512", "tma"),
           ("COM128", "wide"), ("NOC1", "wide"), ("AXC", "wide"), ("CSR", "wide")]
 KIDS = {"ldg": 1, "tma": 2, "rows": 3, "wide": 4}
-WIDE_VARIANTS = list(range(16))
+WIDE_VARIANTS = list(range(18))
 
 
 @pytest.fixture(scope="module")
@@ -152,7 +152,7 @@ def test_wide_rejects_other_forms(env):
         make_plan(F, D, csr, g["x"], "COM128", val="f32lo", kernel="wide")
 
 
-WIDE_D16 = [0, 4, 8, 9, 14, 15]
+WIDE_D16 = [0, 4, 8, 9, 14, 15, 16, 17]
 
 
 @pytest.mark.parametrize("fmt", ["COM128", "NOC1", "CSR"])
@@ -169,7 +169,7 @@ def test_wide_d16(env, fmt, variant, val_kind):
         x = M.uniform_x(len(row) - 1, 30 + i)
         for beta in (0, 1):
             p, _ = check_plan(env, row, col, val, x, fmt, val_kind, beta, kernel="wide", variant=variant, col="d16")
-            assert p.info["kernel"] == 4 and p.info["col_kind"] == 1 and p.kernel_name().endswith("d16>")
+            assert p.info["kernel"] == 4 and p.info["col_kind"] == 1 and "d16" in p.kernel_name()
 
 
 @pytest.mark.parametrize("fmt", ["COM128", "NOC1"])
@@ -179,11 +179,14 @@ def test_auto_picks_wide(env, fmt):
     BF16 lo-word form keeps stream_ldg."""
     torch, D, F, orc = env
     from int_spmv_b200 import matrices as M
-    for rl_max, spl in ((8, "<8,"), (60, "<16,")):
+    for rl_max, name in ((8, "stream_wide<8,"), (60, "stream_wide_tma<16,")):
         row, col, val = M.random_csr(5000, rl_max, rl_max=rl_max, empty_frac=0.05)
         x = M.uniform_x(5000, rl_max)
         p, _ = check_plan(env, row, col, val, x, fmt)
-        assert p.info["kernel"] == 4 and p.kernel_name().startswith("stream_wide" + spl)
+        assert p.info["kernel"] == 4 and p.kernel_name().startswith(name)
+        if rl_max > 8:
+            p, _ = check_plan(env, row, col, val, x, fmt, val_kind="f32")
+            assert p.kernel_name().startswith("stream_wide<16,")
         p, _ = check_plan(env, row, col, val, x, fmt, col="d16")
         assert p.info["kernel"] == 4 and p.kernel_name().endswith("d16>")
         p, _ = check_plan(env, row, col, val, x, fmt, val_kind="f32lo")
@@ -314,3 +317,37 @@ def test_kernel_timing_events(env, fmt, kernel):
     torch.cuda.synchronize()
     assert p.kernel_ms() == (0.0, 0)
     assert_parity(y.cpu().numpy(), orc.cf_csr(row, col, val, x), orc.abs_csr(row, col, val, x), TOL_F64)
+
+
+@pytest.mark.parametrize("val_kind", ["f64", "f32"])
+def test_wide_texture_gathers_and_fallback(env, val_kind):
+    """Texture-gather variants: an aligned x is fetched through a linear
+    texture; an x that does not meet the texture alignment (a view 8 bytes
+    into a buffer) is gathered with loads; both give the oracle's product."""
+    torch, D, F, orc = env
+    from int_spmv_b200 import matrices as M
+    row, col, val = M.random_csr(5003, 3, rl_max=40, empty_frac=0.05)
+    x = M.uniform_x(5003, 3)
+    csr = F.CSR(row, col, val)
+    ref, ab = orc.cf_csr(row, col, val, x), orc.abs_csr(row, col, val, x)
+    tol = TOL_F64 if val_kind == "f64" else TOL_F32
+    for variant in (16, 17):
+        p = make_plan(F, D, csr, x, "COM128", kernel="wide", variant=variant, val=val_kind)
+        y = p.spmv(torch.from_numpy(x).cuda()).cpu().numpy()
+        if val_kind == "f64":
+            assert p.kernel_name().endswith("tex>"), p.kernel_name()
+        assert_parity(y, ref, ab, tol, what=f"tex v{variant}")
+        buf = torch.zeros(5004, dtype=torch.float64, device="cuda")
+        buf[1:] = torch.from_numpy(x).cuda()
+        y2 = p.spmv(buf[1:]).cpu().numpy()
+        if val_kind == "f64":
+            assert "gathered with loads" in p.kernel_name(), p.kernel_name()
+        assert_parity(y2, ref, ab, tol, what=f"tex fallback v{variant}")
+        # a captured graph gathers with loads (it must not name a texture a
+        # later product replaces), and later products with other x stay right
+        xa = torch.from_numpy(x).cuda()
+        yg = torch.empty_like(xa)
+        p.spmv_graph(xa, yg)
+        p.spmv(buf[1:])
+        p.spmv_graph(xa, yg)
+        assert_parity(yg.cpu().numpy(), ref, ab, tol, what=f"tex graph v{variant}")
