@@ -264,6 +264,15 @@ int ispmv_dev_axt_free(str_matAXT *m);
 /* Copies a device-built AXT's con/ax/sec (lenCON/lenAX/lenSEC entries) into
  * caller buffers, host or device (NULL skips one); synchronises `stream`. */
 int ispmv_dev_axt_export(const str_matAXT *m, UIN *con, FPT *ax, UIN *sec, void *stream);
+/* getFormatDataK1 (M:841-905) on the GPU, likewise: permi/nmc/chp/val/col
+ * bit for bit the host builder's, from device CSR arrays; device pointers in
+ * the struct (ispmv_dev_k1_free); feed them to ispmv_dev_int_k1 / _k1p. */
+int ispmv_dev_build_k1(UIN n, UIN nnz, const UIN *d_row, const UIN *d_col, const FPT *d_val, str_matK1 *m,
+                       str_formatData *fd, void *stream);
+int ispmv_dev_k1_free(str_matK1 *m);
+/* Copies permi ((chunkNum+1)*8), nmc, chp (chunkNum) and val, col (lenVC)
+ * into caller buffers (NULL skips one); synchronises `stream`. */
+int ispmv_dev_k1_export(const str_matK1 *m, UIN *permi, UIN *nmc, UIN *chp, FPT *val, UIN *col, void *stream);
 
 /* ---------------------------------------------------------------------------
  * Layer 3: plans - a format resident in HBM as value/column streams; every
@@ -319,7 +328,10 @@ int ispmv_plan_axt(const str_matCSR *csr, const str_matAXT *axt, const UIN *axi,
                    const ispmv_plan_opts *o, ispmv_plan *out);
 int ispmv_plan_destroy(ispmv_plan p);
 
-/* y = A*x + beta*y with device pointers, beta in {0, 1}.  Stream-ordered. */
+/* y = A*x + beta*y with device pointers, beta in {0, 1}.  Stream-ordered.
+ * A plan keeps per-product work areas on the device (segment records, the
+ * FP32 copy of x of FP32-value plans): use one plan on one stream at a time;
+ * products on two streams that overlap need two plans. */
 int ispmv_plan_spmv(ispmv_plan p, const FPT *x, FPT *y, int beta, void *stream);
 /* The same product as one CUDA-graph launch: the plan captures its kernels
  * (queue reset, SpMV, row fix-up) for this (x, y, beta) on first use, and

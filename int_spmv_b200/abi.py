@@ -73,6 +73,9 @@ PROTOTYPES: dict[str, tuple] = {
                                       C.POINTER(StrMatAXT), C.POINTER(StrFormatData), VP]),
     "ispmv_dev_axt_free": (C.c_int, [C.POINTER(StrMatAXT)]),
     "ispmv_dev_axt_export": (C.c_int, [C.POINTER(StrMatAXT), VP, VP, VP, VP]),
+    "ispmv_dev_build_k1": (C.c_int, [UIN, UIN, VP, VP, VP, C.POINTER(StrMatK1), C.POINTER(StrFormatData), VP]),
+    "ispmv_dev_k1_free": (C.c_int, [C.POINTER(StrMatK1)]),
+    "ispmv_dev_k1_export": (C.c_int, [C.POINTER(StrMatK1), VP, VP, VP, VP, VP, VP]),
     # self-test of the bounded device wait
     "ispmv_selftest_bounded_wait": (C.c_int, [C.POINTER(C.c_double), C.c_void_p]),
     # host: statistics, files, builders

@@ -15,9 +15,17 @@
 // Steps: row slot counts -> exclusive prefix (three scan kernels over u64)
 // -> sizes read back to the host (one synchronisation, to allocate) ->
 // one warp per row writes its slots.
+//
+// The K1 arrays of getFormatDataK1 (M:841-905) likewise: rows sorted by
+// length, descending, equal lengths in ascending row order (the order of the
+// reference's qsort, M:775-796) by a stable radix sort (CUB, builder only);
+// nmc[c] = the length of chunk c's first row, chp = the exclusive prefix of
+// 8*nmc; val/col column-major per chunk, zero padding.
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+
+#include <cub/device/device_radix_sort.cuh>
 
 #include "common.cuh"
 
@@ -155,6 +163,43 @@ __global__ void __launch_bounds__(256) fill_axt(UIN n, const UIN *__restrict__ r
   }
 }
 
+__global__ void row_lengths(UIN n, const UIN *__restrict__ row, UIN *__restrict__ rl, UIN *__restrict__ ids) {
+  const size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  rl[r] = row[r + 1] - row[r];
+  ids[r] = (UIN)r;
+}
+
+// chunk c: nmc = its first row's length; cnt = 8*nmc (scanned into chp)
+__global__ void chunk_widths(UIN cn, const UIN *__restrict__ rl_sorted, UIN *__restrict__ nmc,
+                             uint64_t *__restrict__ cnt) {
+  const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c > cn) return;
+  if (c == cn) {
+    cnt[cn] = 0;
+    return;
+  }
+  nmc[c] = rl_sorted[c * 8];
+  cnt[c] = 8ull * rl_sorted[c * 8];
+}
+
+// One thread per (chunk, lane): the row's elements go down the chunk column.
+__global__ void fill_k1(UIN n, const UIN *__restrict__ row, const UIN *__restrict__ col, const FPT *__restrict__ val,
+                        const UIN *__restrict__ permi, const uint64_t *__restrict__ chp64, UIN *__restrict__ chp,
+                        FPT *__restrict__ kval, UIN *__restrict__ kcol) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const size_t c = i / 8, lane = i % 8;
+  const UIN base = (UIN)chp64[c];
+  if (lane == 0) chp[c] = base;
+  const UIN r = permi[i], j0 = row[r], len = row[r + 1] - j0;
+  for (UIN k = 0; k < len; k++) {
+    const size_t p = (size_t)base + (size_t)k * 8 + lane;
+    kval[p] = val[j0 + k];
+    kcol[p] = col[j0 + k];
+  }
+}
+
 UIN floor_log2_lt1024(UIN v) {  // M:1286-1287 / M:1341-1348: the largest i < 10 with (v >> i) == 1
   UIN r = 0;
   for (UIN i = 0; i < 10; i++)
@@ -285,5 +330,131 @@ done:
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
   if (st != ISPMV_OK) ispmv_dev_axt_free(m);
+  return st;
+}
+
+// ---------------------------------------------------------------- K1 --
+ISPMV_API int ispmv_dev_k1_free(str_matK1 *m) {
+  if (!m) return ISPMV_ERR_ARG;
+  cudaFree(m->permi);
+  cudaFree(m->nmc);
+  cudaFree(m->chp);
+  cudaFree(m->val);
+  cudaFree(m->col);
+  std::memset(m, 0, sizeof *m);
+  return ISPMV_OK;
+}
+
+// Copies a device-built K1's arrays into caller buffers (host or device;
+// NULL skips one): permi (chunkNum+1)*8, nmc and chp chunkNum, val and col
+// lenVC entries.  Synchronises `stream`.
+ISPMV_API int ispmv_dev_k1_export(const str_matK1 *m, UIN *permi, UIN *nmc, UIN *chp, FPT *val, UIN *col,
+                                  void *stream) {
+  if (!m) return ISPMV_ERR_ARG;
+  cudaStream_t s = as_stream(stream);
+  const size_t cn = m->chunkNum;
+  if (permi) ISPMV_TRY(cudaMemcpyAsync(permi, m->permi, (cn + 1) * 8 * sizeof(UIN), cudaMemcpyDefault, s));
+  if (nmc && cn) ISPMV_TRY(cudaMemcpyAsync(nmc, m->nmc, cn * sizeof(UIN), cudaMemcpyDefault, s));
+  if (chp && cn) ISPMV_TRY(cudaMemcpyAsync(chp, m->chp, cn * sizeof(UIN), cudaMemcpyDefault, s));
+  if (val && m->lenVC) ISPMV_TRY(cudaMemcpyAsync(val, m->val, (size_t)m->lenVC * sizeof(FPT), cudaMemcpyDefault, s));
+  if (col && m->lenVC) ISPMV_TRY(cudaMemcpyAsync(col, m->col, (size_t)m->lenVC * sizeof(UIN), cudaMemcpyDefault, s));
+  ISPMV_TRY(cudaStreamSynchronize(s));
+  return ISPMV_OK;
+}
+
+// getFormatDataK1 on the GPU from device CSR arrays; the struct's arrays
+// come back as device pointers (ispmv_dev_k1_free); fd->ct is the GPU time.
+ISPMV_API int ispmv_dev_build_k1(UIN n, UIN nnz, const UIN *d_row, const UIN *d_col, const FPT *d_val, str_matK1 *m,
+                                 str_formatData *fd, void *stream) {
+  if (!m || !d_row || n == 0 || (nnz && (!d_col || !d_val))) return ISPMV_ERR_ARG;
+  cudaStream_t s = as_stream(stream);
+  std::memset(m, 0, sizeof *m);
+  const UIN cn = (n + 7) / 8;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  UIN *rl = nullptr, *rls = nullptr, *ids = nullptr;
+  uint64_t *cnt = nullptr, *off = nullptr, *bsum = nullptr;
+  void *tmp = nullptr;
+  size_t tmp_bytes = 0;
+  int st = ISPMV_OK;
+  const size_t len = (size_t)cn + 1, nb = (len + SB - 1) / SB;
+  uint64_t lenVC = 0;
+#define DB_TRY(expr)                \
+  do {                              \
+    cudaError_t e__ = (expr);       \
+    if (e__ != cudaSuccess) {       \
+      st = cuda_status(e__, #expr); \
+      goto done;                    \
+    }                               \
+  } while (0)
+  DB_TRY(cudaEventCreate(&e0));
+  DB_TRY(cudaEventCreate(&e1));
+  DB_TRY(cudaMalloc(&rl, (size_t)n * sizeof(UIN)));
+  DB_TRY(cudaMalloc(&rls, ((size_t)cn * 8) * sizeof(UIN)));
+  DB_TRY(cudaMalloc(&ids, (size_t)n * sizeof(UIN)));
+  DB_TRY(cudaMalloc(&m->permi, ((size_t)cn + 1) * 8 * sizeof(UIN)));
+  DB_TRY(cudaMalloc(&m->nmc, std::max<size_t>(1, cn) * sizeof(UIN)));
+  DB_TRY(cudaMalloc(&m->chp, std::max<size_t>(1, cn) * sizeof(UIN)));
+  DB_TRY(cudaMalloc(&cnt, len * sizeof(uint64_t)));
+  DB_TRY(cudaMalloc(&off, len * sizeof(uint64_t)));
+  DB_TRY(cudaMalloc(&bsum, nb * sizeof(uint64_t)));
+  DB_TRY(cub::DeviceRadixSort::SortPairsDescending(nullptr, tmp_bytes, rl, rls, ids, m->permi, (int)n, 0,
+                                                   32, s));
+  DB_TRY(cudaMalloc(&tmp, std::max<size_t>(1, tmp_bytes)));
+  DB_TRY(cudaEventRecord(e0, s));
+  DB_TRY(cudaMemsetAsync(m->permi, 0, ((size_t)cn + 1) * 8 * sizeof(UIN), s));  // zero beyond n (M:851-852)
+  DB_TRY(cudaMemsetAsync(rls, 0, (size_t)cn * 8 * sizeof(UIN), s));
+  row_lengths<<<(unsigned)(((size_t)n + 255) / 256), 256, 0, s>>>(n, d_row, rl, ids);
+  if ((st = check_launch("row_lengths"))) goto done;
+  // stable: equal lengths keep ascending row ids
+  DB_TRY(cub::DeviceRadixSort::SortPairsDescending(tmp, tmp_bytes, rl, rls, ids, m->permi, (int)n, 0, 32, s));
+  chunk_widths<<<(unsigned)((len + 255) / 256), 256, 0, s>>>(cn, rls, m->nmc, cnt);
+  if ((st = check_launch("chunk_widths"))) goto done;
+  scan_block<<<(unsigned)nb, ST, 0, s>>>(len, cnt, off, bsum);
+  if ((st = check_launch("scan_block"))) goto done;
+  scan_totals<<<1, ST, 0, s>>>(nb, bsum);
+  if ((st = check_launch("scan_totals"))) goto done;
+  add_block_offsets<<<(unsigned)((len + 255) / 256), 256, 0, s>>>(len, off, bsum);
+  if ((st = check_launch("add_block_offsets"))) goto done;
+  DB_TRY(cudaMemcpyAsync(&lenVC, off + cn, sizeof lenVC, cudaMemcpyDeviceToHost, s));
+  DB_TRY(cudaStreamSynchronize(s));
+  if (lenVC > 0xFFFFFFFFull) {
+    st = ISPMV_ERR_OVERFLOW;
+    goto done;
+  }
+  m->nrows = n;
+  m->nnz = nnz;
+  m->chunkNum = cn;
+  m->lenVC = (UIN)lenVC;
+  DB_TRY(cudaMalloc(&m->val, std::max<uint64_t>(1, lenVC) * sizeof(FPT)));
+  DB_TRY(cudaMalloc(&m->col, std::max<uint64_t>(1, lenVC) * sizeof(UIN)));
+  DB_TRY(cudaMemsetAsync(m->val, 0, lenVC * sizeof(FPT), s));
+  DB_TRY(cudaMemsetAsync(m->col, 0, lenVC * sizeof(UIN), s));
+  fill_k1<<<(unsigned)(((size_t)n + 255) / 256), 256, 0, s>>>(n, d_row, d_col, d_val, m->permi, off, m->chp, m->val,
+                                                               m->col);
+  if ((st = check_launch("fill_k1"))) goto done;
+  DB_TRY(cudaEventRecord(e1, s));
+  DB_TRY(cudaEventSynchronize(e1));
+  if (fd) {
+    float ms = 0.f;
+    DB_TRY(cudaEventElapsedTime(&ms, e0, e1));
+    std::memset(fd, 0, sizeof *fd);
+    std::snprintf(fd->name, sizeof fd->name, "K1");
+    fd->mfp = 2.0 * cn * sizeof(UIN) + (double)m->lenVC * (sizeof(FPT) + sizeof(UIN)) + (double)n * sizeof(UIN) +
+              (double)n * sizeof(FPT);
+    fd->beta = m->lenVC ? (double)nnz / (double)m->lenVC : 0.0;
+    fd->ct = ms * 1e-3;
+  }
+#undef DB_TRY
+done:
+  cudaFree(rl);
+  cudaFree(rls);
+  cudaFree(ids);
+  cudaFree(cnt);
+  cudaFree(off);
+  cudaFree(bsum);
+  cudaFree(tmp);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (st != ISPMV_OK) ispmv_dev_k1_free(m);
   return st;
 }

@@ -257,3 +257,49 @@ class DeviceAXT:
             check(lib.ispmv_dev_int_axt_com_h1(bn, bs, c.log, c.tileHW, c.tileN, c.lenAX, c.lenSEC, ax, sec, _ptr(y),
                                                _stream(stream)), "ispmv_dev_int_axt_com_h1")
         return y
+
+
+class DeviceK1:
+    """getFormatDataK1 (intSpmv_main.c:841) run on the GPU
+    (ispmv_dev_build_k1): permi, nmc, chp, val and col of the K1 format, bit
+    for bit the host builder's, from CSR arrays on the device; the arrays stay
+    in device memory (owned here)."""
+
+    def __init__(self, row: torch.Tensor, col: torch.Tensor, val: torch.Tensor, stream=None):
+        lib = load()
+        n, nnz = row.numel() - 1, col.numel()
+        self.c, self.fd = abi.StrMatK1(), abi.StrFormatData()
+        check(lib.ispmv_dev_build_k1(n, nnz, _ptr(row), _ptr(col) if nnz else None, _ptr(val) if nnz else None,
+                                     C.byref(self.c), C.byref(self.fd), _stream(stream)), "ispmv_dev_build_k1")
+
+    def __del__(self):
+        c = getattr(self, "c", None)
+        if c is not None and c.permi:
+            try:
+                load().ispmv_dev_k1_free(C.byref(c))
+            except Exception:
+                pass
+
+    @property
+    def conversion_s(self) -> float:
+        return float(self.fd.ct)
+
+    def to_host(self, stream=None) -> dict:
+        cn, lv = self.c.chunkNum, self.c.lenVC
+        a = dict(permi=np.zeros((cn + 1) * 8, np.uint32), nmc=np.zeros(cn, np.uint32), chp=np.zeros(cn, np.uint32),
+                 val=np.zeros(lv, np.float64), col=np.zeros(lv, np.uint32))
+        ptr = {k: (v.ctypes.data or None) for k, v in a.items()}
+        check(load().ispmv_dev_k1_export(C.byref(self.c), ptr["permi"], ptr["nmc"], ptr["chp"], ptr["val"],
+                                         ptr["col"], _stream(stream)), "ispmv_dev_k1_export")
+        return a
+
+    def spmv(self, x: torch.Tensor, y: torch.Tensor, stream=None) -> torch.Tensor:
+        """int_k1p (K1 with integrated reordering, intSpmv_main.c:1026) on
+        the device arrays: y[permi[i]] = row i of the chunk order."""
+        c = self.c
+        rem = c.nrows - 8 * (c.chunkNum - 1)
+        mask = (1 << rem) - 1
+        vp = lambda q: C.cast(q, C.c_void_p)  # noqa: E731
+        check(load().ispmv_dev_int_k1p(mask, c.chunkNum, vp(c.val), vp(c.col), vp(c.chp), vp(c.nmc), vp(c.permi),
+                                       _ptr(x), _ptr(y), _stream(stream)), "ispmv_dev_int_k1p")
+        return y
