@@ -26,6 +26,7 @@
 #include "plan_tma.cuh"
 #include "spmm.cuh"
 #include "sss.cuh"
+#include "tmem.cuh"
 #include "wide.cuh"
 
 using namespace ispmv;
@@ -62,6 +63,7 @@ struct ispmv_plan_s {
   cudaTextureObject_t xtex = 0;      // linear texture over x (stream_wide texture-gather variants)
   const void *xtex_src = nullptr;    // the buffer it covers
   size_t xtex_bytes = 0;
+  uint32_t *tblocks = nullptr;       // the stream in TMEM-staged blocks (stream_tmem variants)
   unsigned long long *queue = nullptr;  // work-queue counter (variant ISPMV_VARIANT_QUEUE)
   cudaStream_t cap_stream = nullptr;    // private stream for graph capture
   cudaGraph_t graph = nullptr;
@@ -237,6 +239,8 @@ bool xw_variant(int v, XwCfg *c) {
 // staged form (tma) the stages per warp and warps per CTA.
 struct WideCfg {
   int spl; bool win; UIN cap; size_t seg; int minb; bool buf; bool tma; int stages; int warps; bool tex = false;
+  bool tmem = false;  // stream staged through tensor memory (stream_tmem); stages = TMEM stages,
+                      // warps = consumer warps per CTA (4 per column half)
 };
 constexpr int WIDE_WARPS = 8;
 WideCfg wide_variant(int v) {
@@ -258,6 +262,10 @@ WideCfg wide_variant(int v) {
     case 15: return {16, false, 0, 8192, 2, false, false, 0, 8};
     case 16: return {8, false, 0, 2048, 4, false, false, 0, 8, true};   // texture gathers
     case 17: return {16, false, 0, 4096, 3, false, false, 0, 8, true};
+    case 18: return {8, false, 0, 8192, 0, false, false, 4, 4, false, true};   // TMEM-staged stream
+    case 19: return {16, false, 0, 8192, 0, false, false, 2, 4, false, true};
+    case 20: return {8, false, 0, 8192, 0, false, false, 2, 8, false, true};
+    case 21: return {16, false, 0, 8192, 0, false, false, 2, 8, false, true};
     default: return {16, false, 0, 4096, 3, false, false, 0, 8};
   }
 }
@@ -309,6 +317,11 @@ int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v,
                  const std::vector<size_t> &start) {
   p->path = P_STREAM;
   p->slots_pad = std::max(SS, (p->slots + SS - 1) / SS * SS);
+  if (p->opts.kernel == ISPMV_KERNEL_WIDE && wide_variant(p->opts.variant).tmem) {
+    // whole CTAs: every consumer warp of stream_tmem walks a full segment
+    const size_t unit = (size_t)wide_variant(p->opts.variant).warps * wide_variant(p->opts.variant).seg;
+    p->slots_pad = std::max(unit, (p->slots + unit - 1) / unit * unit);
+  }
   v.resize(p->slots_pad, 0.0);
   c.resize(p->slots_pad, 0);
   std::vector<UIN> heads(p->slots_pad / 32, 0), rowmap;
@@ -327,14 +340,15 @@ int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v,
   const bool wide = p->opts.kernel == ISPMV_KERNEL_WIDE;
   if (wide) {
     const WideCfg wc = wide_variant(p->opts.variant);
-    if (p->opts.val_kind == ISPMV_VAL_F32_LO16 || (p->opts.col_kind == ISPMV_COL_D16 && (wc.win || wc.tma || wc.buf)))
+    if (p->opts.val_kind == ISPMV_VAL_F32_LO16 ||
+        (p->opts.col_kind == ISPMV_COL_D16 && (wc.win || wc.tma || wc.buf || wc.tmem)))
       return fail(ISPMV_ERR_UNSUPPORTED,
                   "stream_wide: FP64/FP32 values; 16-bit column deltas on the plain-load variants without x bands");
     xc = {wc.warps, wc.cap, wc.seg};
     xwv = wc.win;
   }
   p->seg_slots = xwv && p->opts.units_per_warp <= 0 ? xc.seg : seg_slots_of(p, 1);
-  if (wide && p->opts.units_per_warp <= 0) p->seg_slots = xc.seg;
+  if (wide && (p->opts.units_per_warp <= 0 || wide_variant(p->opts.variant).tmem)) p->seg_slots = xc.seg;
   if (wide && p->seg_slots % SS) p->seg_slots = (p->seg_slots + SS - 1) / SS * SS;
   p->nseg = (p->slots_pad + p->seg_slots - 1) / p->seg_slots;
   std::vector<UIN> segh(std::max<size_t>(1, p->nseg), 0);
@@ -344,7 +358,40 @@ int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v,
     for (; w < wend; w++) acc += __builtin_popcount(heads[w]);
     segh[sg] = acc;
   }
-  if (wide) {
+  if (wide && wide_variant(p->opts.variant).tmem) {
+    // TMEM-staged blocks: block j of CTA c holds batch j of segments
+    // nw*c..nw*c+nw-1, one half-block per 4 of them; in half-block h,
+    // lane-row r = 32q + l (segment nw*c + 4h + q, lane l) with its SPL values
+    // then its SPL columns, in the copy's canonical layout (tmemk::blk_word)
+    const unsigned spl = (unsigned)wide_variant(p->opts.variant).spl, BT = 32u * spl;
+    const unsigned nw = (unsigned)wide_variant(p->opts.variant).warps;  // 4 per column half
+    const bool f64 = p->opts.val_kind == ISPMV_VAL_F64;
+    const unsigned vw = f64 ? 2u : 1u, W = vw * spl + spl, BW = W / 8u * 1024u;  // words per half-block
+    const size_t nbat = p->seg_slots / BT, nctas = p->nseg / nw;
+    std::vector<uint32_t> blk(nctas * nbat * BW * (nw / 4u), 0u);
+    for (size_t cta = 0; cta < nctas; cta++)
+      for (size_t j = 0; j < nbat; j++)
+        for (unsigned w = 0; w < nw; w++) {
+          uint32_t *B = blk.data() + ((cta * nbat + j) * (nw / 4u) + w / 4u) * BW;
+          const unsigned q = w % 4u;
+          for (unsigned l = 0; l < 32u; l++)
+            for (unsigned k = 0; k < spl; k++) {
+              const size_t sl = (cta * nw + w) * p->seg_slots + j * BT + (size_t)spl * l + k;
+              const unsigned r = 32u * q + l;
+              if (f64) {
+                uint64_t u;
+                std::memcpy(&u, &v[sl], 8);
+                B[tmemk::blk_word(r, 2u * k)] = (uint32_t)u;
+                B[tmemk::blk_word(r, 2u * k + 1u)] = (uint32_t)(u >> 32);
+              } else {
+                const float f = (float)v[sl];
+                std::memcpy(&B[tmemk::blk_word(r, k)], &f, 4);
+              }
+              B[tmemk::blk_word(r, vw * spl + k)] = c[sl];
+            }
+      }
+    TRY(dev_upload(p, blk.data(), blk.size(), &p->tblocks));
+  } else if (wide) {
     // the lane-interleaved copy: batches of 32*spl slots, one 16-byte vector per lane and step
     const unsigned spl = (unsigned)wide_variant(p->opts.variant).spl;
     std::vector<double> vi(p->slots_pad);
@@ -801,6 +848,29 @@ int launch_wide_tma(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, 
   return check_launch(name);
 }
 
+// The TMEM-staged form: one CTA of 4 consumer warps + 1 producer warp per 4
+// segments.
+template <typename VT, int SPL, int S, int H>
+int launch_tmem(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, const char *name) {
+  const void *xs = x;
+  if constexpr (sizeof(VT) == 4) {  // FP32 values: gather the FP32 copy of x
+    if (!p->x32) TRY(dev_alloc(p, p->n, &p->x32));
+    const unsigned gc = (unsigned)std::min<size_t>(((size_t)p->n / 2 + 255) / 256, (size_t)sm_count() * 8) + 1;
+    if ((reinterpret_cast<uintptr_t>(x) & 15u) == 0) wide::x_to_f32<true><<<gc, 256, 0, s>>>(p->n, x, p->x32);
+    else wide::x_to_f32<false><<<gc, 256, 0, s>>>(p->n, x, p->x32);
+    TRY(check_launch("x_to_f32"));
+    xs = p->x32;
+  }
+  using XT = typename std::conditional<sizeof(VT) == 4, float, double>::type;
+  auto *k = tmemk::stream_tmem<VT, XT, SPL, S, H>;
+  const size_t smem = tmemk::smem_bytes<VT, SPL, S, H>();
+  ISPMV_TRY(cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  const unsigned g = (unsigned)(p->nseg / (tmemk::CW * H));
+  k<<<g, (tmemk::CW * H + 1) * 32, smem, s>>>(p->slots, p->seg_slots, p->tblocks, p->heads, p->segh,
+                                               static_cast<const XT *>(xs), o, p->status);
+  return check_launch(name);
+}
+
 // stream_wide<slots per lane, x bands, CTAs per SM, row buffer> for 0..3 bands.
 #define ISPMV_WIDE_NW(SPL, MINB, BUF)                                                                        \
   switch (nw) {                                                                                              \
@@ -813,6 +883,14 @@ int launch_wide_tma(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, 
 template <typename VT>
 int run_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
   const WideCfg wc = wide_variant(p->opts.variant);
+  if (wc.tmem) {
+    switch (p->opts.variant) {
+      case 18: return launch_tmem<VT, 8, 4, 1>(p, x, o, s, "stream_tmem<8,s4,w4>");
+      case 19: return launch_tmem<VT, 16, 2, 1>(p, x, o, s, "stream_tmem<16,s2,w4>");
+      case 20: return launch_tmem<VT, 8, 2, 2>(p, x, o, s, "stream_tmem<8,s2,w8>");
+      default: return launch_tmem<VT, 16, 2, 2>(p, x, o, s, "stream_tmem<16,s2,w8>");
+    }
+  }
   if (wc.tma) {
     switch (p->opts.variant) {
       case 10: return launch_wide_tma<VT, 8, 3, 8>(p, x, o, s, "stream_wide_tma<8,s3,w8>");
@@ -1175,6 +1253,9 @@ namespace {
 unsigned il_spl(const ispmv_plan_s *p) {
   return p->opts.kernel == ISPMV_KERNEL_WIDE ? (unsigned)wide_variant(p->opts.variant).spl : 0u;
 }
+bool tmem_plan(const ispmv_plan_s *p) {
+  return p->opts.kernel == ISPMV_KERNEL_WIDE && wide_variant(p->opts.variant).tmem;
+}
 
 template <int G, typename VT>
 int spmm_blocks(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
@@ -1214,7 +1295,7 @@ int spmm_run(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
 // (AXT COM, AXT tileH=1, AXC and CSR built with the stream kernels).
 ISPMV_API int ispmv_plan_spmm(ispmv_plan p, UIN k, const FPT *X, FPT *Y, void *stream) {
   if (!p || !X || !Y || k == 0) return ISPMV_ERR_ARG;
-  if (p->path != P_STREAM || narrow_kinds(p))
+  if (p->path != P_STREAM || narrow_kinds(p) || tmem_plan(p))
     return fail(ISPMV_ERR_UNSUPPORTED, "ispmv_plan_spmm: needs a slot-stream plan with u32 columns");
   cudaStream_t s = as_stream(stream);
   if (!p->slots) {  // every row empty

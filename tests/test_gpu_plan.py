@@ -21,7 +21,7 @@ COMBOS = [("CSR", "rows"), ("CSR", "ldg"), ("CSR", "tma"), ("AXC", "rows"), ("AX
           ("COM128", "ldg"), ("COM128", "tma"), ("COM256", "ldg"), ("COM512", "tma"),
           ("COM128", "wide"), ("NOC1", "wide"), ("AXC", "wide"), ("CSR", "wide")]
 KIDS = {"ldg": 1, "tma": 2, "rows": 3, "wide": 4}
-WIDE_VARIANTS = list(range(18))
+WIDE_VARIANTS = list(range(22))
 
 
 @pytest.fixture(scope="module")
@@ -136,7 +136,7 @@ def test_wide_variants(env, fmt, variant, val_kind):
         x = M.uniform_x(len(row) - 1, 12 + i)
         for beta in (0, 1):
             p, _ = check_plan(env, row, col, val, x, fmt, val_kind, beta, kernel="wide", variant=variant)
-            assert p.info["kernel"] == 4 and p.kernel_name().startswith("stream_wide")
+            assert p.info["kernel"] == 4 and p.kernel_name().startswith(("stream_wide", "stream_tmem"))
 
 
 def test_wide_rejects_other_forms(env):
