@@ -412,10 +412,26 @@ def main(argv=None):
                 dv_s.append(dv.conversion_s)
                 del dv
             dv_s = dv_s[-1]
+            # the plan itself (the compacted AXT's lane-interleaved stream)
+            # from the host CSR and from the device CSR, wall clock
+            plan_s = {}
+            t0 = time.perf_counter()
+            ph = D.Plan(csr, None, kernel="wide", variant=4)
+            plan_s["host_s"] = time.perf_counter() - t0
+            del ph
+            for _ in range(2):  # the first call also loads the builder's kernels
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                pdv = D.Plan.from_device_csr(drow, dcol, dval, kernel="wide", variant=4)
+                plan_s["gpu_s"] = time.perf_counter() - t0
+                del pdv
             del drow, dcol, dval
             conversion = {"format": "AXT_COM_H1_HW8_BS128", "host_s": fd_h.ct, "host_threads": os.cpu_count(),
                           "gpu_s": dv_s, "note": "host: getFormatDataAXT (ispmv_build_axt, wall clock); "
-                                                 "gpu: ispmv_dev_build_axt on device CSR + x (CUDA events)"}
+                                                 "gpu: ispmv_dev_build_axt on device CSR + x (CUDA events)",
+                          "plan": dict(plan_s, note="plan of the lane-interleaved stream (variant 4): "
+                                                    "ispmv_plan_csr from host CSR vs ispmv_plan_dev_csr from "
+                                                    "device CSR, wall clock including synchronisation")}
         except Exception as e:
             conversion = {"unavailable": str(e)[:120]}
 

@@ -58,6 +58,11 @@ class PlanInfo(C.Structure):
                 ("kernel", C.c_int), ("tile_h", UIN), ("bs", UIN), ("name", C.c_char * 32)]
 
 
+class PlanLayout(C.Structure):
+    _fields_ = [("slots", C.c_uint64), ("slots_pad", C.c_uint64), ("seg_slots", C.c_uint64), ("nseg", C.c_uint64),
+                ("nrowmap", C.c_uint64), ("nempty", C.c_uint64), ("val_bytes", UIN), ("spl", UIN)]
+
+
 P_CSR = C.POINTER(StrMatCSR)
 P_FD = C.POINTER(StrFormatData)
 P_AXC = C.POINTER(StrMatAXC)
@@ -127,6 +132,9 @@ PROTOTYPES: dict[str, tuple] = {
     "ispmv_plan_axc": (C.c_int, [P_CSR, P_AXC, P_UIN, P_OPTS, P_PLAN]),
     "ispmv_plan_k1": (C.c_int, [P_CSR, P_K1, C.c_int, P_OPTS, P_PLAN]),
     "ispmv_plan_axt": (C.c_int, [P_CSR, P_AXT, P_UIN, P_OPTS, P_PLAN]),
+    "ispmv_plan_dev_csr": (C.c_int, [UIN, UIN, VP, VP, VP, P_OPTS, P_PLAN, VP]),
+    "ispmv_plan_get_layout": (C.c_int, [VP, C.POINTER(PlanLayout)]),
+    "ispmv_plan_export_stream": (C.c_int, [VP, VP, VP, VP, VP, VP, VP, VP]),
     "ispmv_plan_destroy": (C.c_int, [VP]),
     "ispmv_plan_spmv": (C.c_int, [VP, VP, VP, C.c_int, VP]),
     "ispmv_plan_spmv_graph": (C.c_int, [VP, VP, VP, C.c_int, VP]),

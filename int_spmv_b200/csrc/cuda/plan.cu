@@ -23,6 +23,8 @@
 #include <cstring>
 #include <vector>
 
+#include <cub/device/device_scan.cuh>
+
 #include "plan_tma.cuh"
 #include "spmm.cuh"
 #include "sss.cuh"
@@ -47,6 +49,7 @@ struct ispmv_plan_s {
   UIN *rows = nullptr;  // row / brick pointer, or unit rows
   UIN *heads = nullptr, *segh = nullptr, *rowmap = nullptr, *empty = nullptr;
   size_t nempty = 0;
+  size_t nrowmap = 0;   // entries of rowmap (0: no empty rows, no map)
   UIN *chp = nullptr, *nmc = nullptr, *permi = nullptr;
   UIN chunkNum = 0;
   FPT *res = nullptr;  // K1 result in chunk order
@@ -241,6 +244,7 @@ struct WideCfg {
   int spl; bool win; UIN cap; size_t seg; int minb; bool buf; bool tma; int stages; int warps; bool tex = false;
   bool tmem = false;  // stream staged through tensor memory (stream_tmem); stages = TMEM stages,
                       // warps = consumer warps per CTA (4 per column half)
+  bool stg = false;   // one x window per CTA (cap doubles), chosen at plan time, copied by one bulk copy
 };
 constexpr int WIDE_WARPS = 8;
 WideCfg wide_variant(int v) {
@@ -266,6 +270,19 @@ WideCfg wide_variant(int v) {
     case 19: return {16, false, 0, 8192, 0, false, false, 2, 4, false, true};
     case 20: return {8, false, 0, 8192, 0, false, false, 2, 8, false, true};
     case 21: return {16, false, 0, 8192, 0, false, false, 2, 8, false, true};
+    // x bands sized for a CTA span of about 800-1600 rows plus a band of
+    // +/-1000 or more: the near half of a band-split plan
+    case 22: return {8, true, 4096, 1024, 4, false, false, 0, 8};
+    case 23: return {8, true, 6144, 2048, 4, false, false, 0, 8};
+    // a per-CTA x window (the densest interval of the CTA's columns) copied
+    // into shared memory by one bulk copy
+    case 24: return {8, false, 4096, 1024, 4, false, false, 0, 8, false, false, true};
+    case 25: return {8, false, 6144, 2048, 4, false, false, 0, 8, false, false, true};
+    case 26: return {8, false, 3072, 1024, 4, false, false, 0, 8, false, false, true};
+    case 27: return {16, false, 6144, 2048, 3, false, false, 0, 8, false, false, true};
+    case 28: return {8, false, 2048, 512, 4, false, false, 0, 8, false, false, true};
+    case 29: return {8, false, 3072, 512, 4, false, false, 0, 8, false, false, true};
+    case 30: return {8, false, 2560, 1024, 4, false, false, 0, 8, false, false, true};
     default: return {16, false, 0, 4096, 3, false, false, 0, 8};
   }
 }
@@ -311,6 +328,80 @@ void choose_windows(const str_matCSR *csr, UIN cap, double span, sss::XWin *xw) 
   }
 }
 
+// Fraction of a deterministic sample of the nonzeros whose column lies
+// far from the diagonal (|c - r| > 1536, outside a 3072-column window) with
+// no column of the next row within 16 of c + 1: gathers with no locality
+// between neighbouring rows, which the L1 cache cannot share between the
+// lanes of a warp (uniformly scattered columns; not the fixed far offsets
+// of a stencil).  Such matrices gain from the staged per-CTA windows.
+double random_far_fraction(const str_matCSR *csr) {
+  const size_t nnz = csr->nnz, S = std::min<size_t>(nnz, 1u << 16);
+  if (!S) return 0.0;
+  const double stride = (double)nnz / (double)S;
+  size_t far = 0;
+  for (size_t i = 0, r = 0; i < S; i++) {
+    const size_t j = (size_t)(i * stride);
+    while (csr->row[r + 1] <= j) r++;
+    const long long c = csr->col[j];
+    if (std::llabs(c - (long long)r) <= 1536) continue;
+    bool near_next = false;
+    if (r + 1 < csr->nrows)
+      for (UIN k = csr->row[r + 1]; k < csr->row[r + 2] && !near_next; k++)
+        near_next = std::llabs((long long)csr->col[k] - c - 1) <= 16;
+    far += !near_next;
+  }
+  return (double)far / (double)S;
+}
+
+// The per-CTA x windows of the staged stream_wide variants: CTA t walks
+// slots [t*T, (t+1)*T), T = WIDE_WARPS*seg_slots; its window is the
+// cap-long interval of x holding the most of those slots' columns (padding
+// slots excluded), centred on them, clamped to x and started at an even
+// column, so the bulk copy starts on a 16-byte boundary and moves a
+// multiple of 16 bytes, all inside x[0, n rounded down to even).  Columns
+// outside a CTA's window are gathered from x.
+int stage_windows(ispmv_plan_s *p, const std::vector<double> &v, const std::vector<UIN> &c) {
+  const UIN W = wide_variant(p->opts.variant).cap & ~1u, ne = p->n & ~1u;
+  const size_t T = (size_t)WIDE_WARPS * p->seg_slots, nt = std::max<size_t>(1, (p->nseg + WIDE_WARPS - 1) / WIDE_WARPS);
+  std::vector<UIN> lo(nt, 0), len(nt, 0);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (long long t = 0; t < (long long)nt; t++) {
+    if (ne <= W) {  // all of x (but an odd last element) fits
+      len[t] = ne;
+      continue;
+    }
+    const size_t a = (size_t)t * T, e = std::min(p->slots, a + T);
+    std::vector<UIN> cs;
+    cs.reserve(T);
+    for (size_t q = a; q < e; q++)
+      if (v[q] != 0.0) cs.push_back(c[q]);
+    long long l = 0;
+    if (!cs.empty()) {
+      std::sort(cs.begin(), cs.end());
+      size_t best = 0, ba = 0, bb = 1;
+      for (size_t i = 0, j = 0; i < cs.size(); i++) {  // [cs[i], cs[i] + W - 1)
+        if (j < i) j = i;
+        while (j < cs.size() && cs[j] - cs[i] < W - 1) j++;
+        if (j - i > best) { best = j - i; ba = i; bb = j; }
+      }
+      const long long span = (long long)cs[bb - 1] - (long long)cs[ba] + 1;
+      l = (long long)cs[ba] - ((long long)W - span) / 2;
+    }
+    l = std::max(0LL, std::min(l, (long long)(ne - W)));
+    lo[t] = (UIN)l & ~1u;
+    len[t] = W;
+  }
+  UIN *dlo, *dlen;
+  TRY(dev_upload(p, lo.data(), lo.size(), &dlo));
+  TRY(dev_upload(p, len.data(), len.size(), &dlen));
+  p->xw.tlo = dlo;
+  p->xw.tlen = dlen;
+  p->xw.cap = W;
+  p->xw.nwin = 1;
+  p->xw.n = p->n;
+  return ISPMV_OK;
+}
+
 // The stream path: `v`/`c` the slot streams (length p->slots), `start[r]`
 // the first slot of row r (rows with no slot are skipped).
 int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v, std::vector<UIN> &c,
@@ -341,7 +432,7 @@ int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v,
   if (wide) {
     const WideCfg wc = wide_variant(p->opts.variant);
     if (p->opts.val_kind == ISPMV_VAL_F32_LO16 ||
-        (p->opts.col_kind == ISPMV_COL_D16 && (wc.win || wc.tma || wc.buf || wc.tmem)))
+        (p->opts.col_kind == ISPMV_COL_D16 && (wc.win || wc.tma || wc.buf || wc.tmem || wc.stg)))
       return fail(ISPMV_ERR_UNSUPPORTED,
                   "stream_wide: FP64/FP32 values; 16-bit column deltas on the plain-load variants without x bands");
     xc = {wc.warps, wc.cap, wc.seg};
@@ -493,6 +584,9 @@ int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v,
   TRY(dev_upload(p, heads.data(), heads.size(), &p->heads));
   TRY(dev_upload(p, segh.data(), segh.size(), &p->segh));
   if (any_empty) TRY(dev_upload(p, rowmap.data(), rowmap.size(), &p->rowmap));
+  p->nrowmap = any_empty ? rowmap.size() : 0;
+  const bool stg = wide && wide_variant(p->opts.variant).stg;
+  if (stg) TRY(stage_windows(p, v, c));
   if (xwv) {
     const double rows_per_slot = (double)rowmap.size() / (double)std::max<size_t>(1, p->slots);
     choose_windows(csr, xc.cap, rows_per_slot * (double)(xc.warps * p->seg_slots), &p->xw);
@@ -503,7 +597,9 @@ int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v,
   }
   TRY(empty_rows(p, csr));
   TRY(alloc_records(p));
-  p->info.device_bytes = (uint64_t)p->slots_pad * vbytes(p) + p->slots_pad / 8 +
+  if (stg) p->xw.status = p->status;
+  p->info.device_bytes = (uint64_t)(stg ? 8 * ((p->nseg + WIDE_WARPS - 1) / WIDE_WARPS) : 0) +
+                         (uint64_t)p->slots_pad * vbytes(p) + p->slots_pad / 8 +
                          (p->opts.col_kind == ISPMV_COL_D16 ? p->slots_pad * 2 + p->slots_pad / p->d16_batch * 4 +
                                                                  p->esc_batches * p->d16_batch * 4
                                                            : p->slots_pad * 4) +
@@ -564,6 +660,221 @@ ISPMV_API int ispmv_plan_csr(const str_matCSR *csr, const ispmv_plan_opts *o, is
   }
   finish_info(p, "CSR");
   return done(p, st, out);
+}
+
+// ------------------------------------------ plans from a device CSR --
+// The CSR-order slot stream (the compacted AXT's stream) built on the GPU
+// from d_row / d_col / d_val, with the arrays setup_stream builds on the host
+// for a lane-interleaved plan: values and columns interleaved per batch of
+// 32*spl slots (wide::il_pos), zero padding to the stream length, the
+// row-start bitmap, per-segment start counts, the compressed -> real row map
+// (when rows are empty) and the empty-row list.  Row starts are set with
+// atomicOr, so the bitmap does not depend on the order of the writes.
+namespace {
+
+// *bad = 1 if the row pointer decreases, row[0] != 0, row[n] != nnz, or a
+// column is >= n.  Only reads row[0..n] and col[0..nnz).
+__global__ void dcsr_check(UIN n, UIN nnz, const UIN *__restrict__ row, const UIN *__restrict__ col,
+                           int *__restrict__ bad) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x, stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t r = i; r < n; r += stride)
+    if (row[r + 1] < row[r]) *bad = 1;
+  for (size_t j = i; j < nnz; j += stride)
+    if (col[j] >= n) *bad = 1;
+  if (i == 0 && (row[0] != 0 || row[n] != nnz)) *bad = 1;
+}
+
+// flag[r] = 1 for a row with elements; flag[n] = 0, so the exclusive prefix
+// at n is the count of non-empty rows.
+__global__ void dcsr_flags(UIN n, const UIN *__restrict__ row, UIN *__restrict__ flag) {
+  const size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r <= n) flag[r] = r < n && row[r + 1] > row[r] ? 1u : 0u;
+}
+
+// Row-start bits, the compressed -> real map and the empty-row list from the
+// prefix `pos` of the non-empty flags.
+__global__ void dcsr_rows(UIN n, const UIN *__restrict__ row, const UIN *__restrict__ pos, UIN *__restrict__ heads,
+                          UIN *__restrict__ rowmap, UIN *__restrict__ empty) {
+  const size_t r = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n) return;
+  const UIN a = row[r];
+  if (row[r + 1] > a) {
+    atomicOr(&heads[a >> 5], 1u << (a & 31u));
+    if (rowmap) rowmap[pos[r]] = (UIN)r;
+  } else if (empty) {
+    empty[r - pos[r]] = (UIN)r;
+  }
+}
+
+// segh[g] = row starts at slots below g*seg: the non-empty rows r with
+// row[r] < g*seg, i.e. pos[first r with row[r] >= g*seg].
+__global__ void dcsr_segh(size_t nseg, size_t seg, UIN n, const UIN *__restrict__ row, const UIN *__restrict__ pos,
+                          UIN *__restrict__ segh) {
+  const size_t g = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= nseg) return;
+  const uint64_t S = (uint64_t)g * seg;
+  UIN lo = 0, hi = n;  // first r in [0, n) with row[r] >= S, else n
+  while (lo < hi) {
+    const UIN mid = lo + (hi - lo) / 2;
+    if ((uint64_t)row[mid] < S) lo = mid + 1;
+    else hi = mid;
+  }
+  segh[g] = pos[lo];
+}
+
+// The lane-interleaved value and column copies, zero beyond nnz.
+template <typename VT>
+__global__ void dcsr_interleave(size_t nnz, size_t spad, unsigned spl, const UIN *__restrict__ col,
+                                const FPT *__restrict__ val, VT *__restrict__ vi, UIN *__restrict__ ci) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < spad; q += stride) {
+    const bool in = q < nnz;
+    vi[wide::il_pos(q, spl, 16u / (unsigned)sizeof(VT))] = (VT)(in ? val[q] : 0.0);
+    ci[wide::il_pos(q, spl, 4u)] = in ? col[q] : 0u;
+  }
+}
+
+struct DevTmp {  // builder scratch, freed on every exit
+  std::vector<void *> v;
+  ~DevTmp() {
+    for (void *q : v) cudaFree(q);
+  }
+  template <typename T>
+  int alloc(size_t n, T **d) {
+    void *q = nullptr;
+    ISPMV_TRY(cudaMalloc(&q, (n ? n : 1) * sizeof(T)));
+    v.push_back(q);
+    *d = static_cast<T *>(q);
+    return ISPMV_OK;
+  }
+};
+
+int dev_csr_stream(ispmv_plan_s *p, UIN n, UIN nnz, const UIN *row, const UIN *col, const FPT *val, cudaStream_t s) {
+  if (p->opts.kernel == ISPMV_KERNEL_AUTO) {
+    // the compacted AXT's default: 8 slots per lane for rows of fewer than
+    // 16 slots on average, else 16 (bulk-copy staged for FP64 values)
+    p->opts.kernel = ISPMV_KERNEL_WIDE;
+    if (p->opts.variant == 0) {
+      const bool long_rows = (double)nnz >= 16.0 * (double)n;
+      p->opts.variant = !long_rows ? 4 : p->opts.val_kind == ISPMV_VAL_F64 ? 11 : 0;
+    }
+  }
+  const WideCfg wc = wide_variant(p->opts.variant);
+  if (p->opts.kernel != ISPMV_KERNEL_WIDE || p->opts.val_kind == ISPMV_VAL_F32_LO16 ||
+      p->opts.col_kind != ISPMV_COL_U32 || wc.win || wc.tmem || wc.stg)
+    return fail(ISPMV_ERR_UNSUPPORTED,
+                "plan from a device CSR: the lane-interleaved kernel (no x bands, windows or TMEM staging), "
+                "FP64/FP32 values, u32 columns");
+  p->fmt = F_CSR;
+  p->path = P_STREAM;
+  p->n = n;
+  p->nnz = nnz;
+  p->slots = nnz;
+  p->slots_pad = std::max(SS, (p->slots + SS - 1) / SS * SS);
+  p->seg_slots = p->opts.units_per_warp <= 0 ? wc.seg : seg_slots_of(p, 1);
+  if (p->seg_slots % SS) p->seg_slots = (p->seg_slots + SS - 1) / SS * SS;
+  p->nseg = (p->slots_pad + p->seg_slots - 1) / p->seg_slots;
+  DevTmp tmp;
+  int *bad;
+  UIN *flag, *pos;
+  TRY(tmp.alloc(1, &bad));
+  TRY(tmp.alloc((size_t)n + 1, &flag));
+  TRY(tmp.alloc((size_t)n + 1, &pos));
+  ISPMV_TRY(cudaMemsetAsync(bad, 0, sizeof(int), s));
+  const unsigned gchk = (unsigned)std::min<size_t>(((size_t)std::max(n, nnz) + 255) / 256, (size_t)sm_count() * 16);
+  dcsr_check<<<std::max(1u, gchk), 256, 0, s>>>(n, nnz, row, col, bad);
+  TRY(check_launch("dcsr_check"));
+  dcsr_flags<<<(unsigned)(((size_t)n + 1 + 255) / 256), 256, 0, s>>>(n, row, flag);
+  TRY(check_launch("dcsr_flags"));
+  size_t tb = 0;
+  ISPMV_TRY(cub::DeviceScan::ExclusiveSum(nullptr, tb, flag, pos, (int)n + 1, s));
+  void *tst;
+  TRY(tmp.alloc(tb, reinterpret_cast<unsigned char **>(&tst)));
+  ISPMV_TRY(cub::DeviceScan::ExclusiveSum(tst, tb, flag, pos, (int)n + 1, s));
+  int hbad = 0;
+  UIN nonempty = 0;
+  ISPMV_TRY(cudaMemcpyAsync(&hbad, bad, sizeof hbad, cudaMemcpyDeviceToHost, s));
+  ISPMV_TRY(cudaMemcpyAsync(&nonempty, pos + n, sizeof nonempty, cudaMemcpyDeviceToHost, s));
+  ISPMV_TRY(cudaStreamSynchronize(s));
+  if (hbad) return fail(ISPMV_ERR_ARG, "plan from a device CSR: malformed row pointer or a column >= n");
+  const unsigned spl = (unsigned)wc.spl;
+  void *vi;
+  if (p->opts.val_kind == ISPMV_VAL_F64) TRY(dev_alloc(p, p->slots_pad, reinterpret_cast<double **>(&vi)));
+  else TRY(dev_alloc(p, p->slots_pad, reinterpret_cast<float **>(&vi)));
+  p->val = vi;
+  TRY(dev_alloc(p, p->slots_pad, &p->col));
+  TRY(dev_alloc(p, p->slots_pad / 32, &p->heads));
+  TRY(dev_alloc(p, std::max<size_t>(1, p->nseg), &p->segh));
+  p->nempty = n - nonempty;
+  p->nrowmap = p->nempty ? nonempty : 0;
+  if (p->nempty) {
+    TRY(dev_alloc(p, p->nrowmap, &p->rowmap));
+    TRY(dev_alloc(p, p->nempty, &p->empty));
+  }
+  ISPMV_TRY(cudaMemsetAsync(p->heads, 0, p->slots_pad / 32 * sizeof(UIN), s));
+  const unsigned gi = (unsigned)std::min<size_t>((p->slots_pad + 255) / 256, (size_t)sm_count() * 32);
+  if (p->opts.val_kind == ISPMV_VAL_F64)
+    dcsr_interleave<double><<<gi, 256, 0, s>>>(nnz, p->slots_pad, spl, col, val, static_cast<double *>(vi), p->col);
+  else
+    dcsr_interleave<float><<<gi, 256, 0, s>>>(nnz, p->slots_pad, spl, col, val, static_cast<float *>(vi), p->col);
+  TRY(check_launch("dcsr_interleave"));
+  dcsr_rows<<<(unsigned)(((size_t)n + 255) / 256), 256, 0, s>>>(n, row, pos, p->heads, p->rowmap, p->empty);
+  TRY(check_launch("dcsr_rows"));
+  dcsr_segh<<<(unsigned)((p->nseg + 255) / 256), 256, 0, s>>>(p->nseg, p->seg_slots, n, row, pos, p->segh);
+  TRY(check_launch("dcsr_segh"));
+  TRY(alloc_records(p));
+  ISPMV_TRY(cudaStreamSynchronize(s));
+  p->info.device_bytes = (uint64_t)p->slots_pad * (vbytes(p) + 4) + p->slots_pad / 8;
+  return ISPMV_OK;
+}
+
+}  // namespace
+
+ISPMV_API int ispmv_plan_dev_csr(UIN n, UIN nnz, const UIN *d_row, const UIN *d_col, const FPT *d_val,
+                                 const ispmv_plan_opts *o, ispmv_plan *out, void *stream) {
+  if (!out || !d_row || n == 0 || (nnz && (!d_col || !d_val))) return ISPMV_ERR_ARG;
+  if ((uint64_t)nnz + sss::SS > 0xFFFFFFFFull) return ISPMV_ERR_OVERFLOW;  // slot ids stay in 32 bits
+  ispmv_plan_s *p;
+  TRY(begin(o, &p));
+  const int st = dev_csr_stream(p, n, nnz, d_row, d_col, d_val, as_stream(stream));
+  finish_info(p, "CSR");
+  return done(p, st, out);
+}
+
+ISPMV_API int ispmv_plan_get_layout(ispmv_plan p, ispmv_plan_layout *l) {
+  if (!p || !l) return ISPMV_ERR_ARG;
+  if (p->path != P_STREAM || p->opts.col_kind != ISPMV_COL_U32 ||
+      (p->opts.kernel == ISPMV_KERNEL_WIDE && wide_variant(p->opts.variant).tmem))
+    return ISPMV_ERR_UNSUPPORTED;
+  std::memset(l, 0, sizeof *l);
+  l->slots = p->slots;
+  l->slots_pad = p->slots_pad;
+  l->seg_slots = p->seg_slots;
+  l->nseg = p->nseg;
+  l->nrowmap = p->nrowmap;
+  l->nempty = p->nempty;
+  l->val_bytes = (UIN)vbytes(p);
+  l->spl = p->opts.kernel == ISPMV_KERNEL_WIDE ? (UIN)wide_variant(p->opts.variant).spl : 0u;
+  return ISPMV_OK;
+}
+
+ISPMV_API int ispmv_plan_export_stream(ispmv_plan p, void *val, UIN *col, UIN *heads, UIN *segh, UIN *rowmap,
+                                       UIN *empty, void *stream) {
+  ispmv_plan_layout l;
+  TRY(ispmv_plan_get_layout(p, &l));
+  cudaStream_t s = as_stream(stream);
+  auto cp = [&](void *dst, const void *src, size_t bytes) -> int {
+    if (dst && src && bytes) ISPMV_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s));
+    return ISPMV_OK;
+  };
+  TRY(cp(val, p->val, l.slots_pad * l.val_bytes));
+  TRY(cp(col, p->col, l.slots_pad * sizeof(UIN)));
+  TRY(cp(heads, p->heads, l.slots_pad / 32 * sizeof(UIN)));
+  TRY(cp(segh, p->segh, l.nseg * sizeof(UIN)));
+  TRY(cp(rowmap, p->rowmap, l.nrowmap * sizeof(UIN)));
+  TRY(cp(empty, p->empty, l.nempty * sizeof(UIN)));
+  ISPMV_TRY(cudaStreamSynchronize(s));
+  return ISPMV_OK;
 }
 
 // ---------------------------------------------------------------- AXC --
@@ -683,7 +994,9 @@ ISPMV_API int ispmv_plan_axt(const str_matCSR *csr, const str_matAXT *axt, const
         if (p->opts.variant == 0) {
           const bool long_rows = (double)p->slots >= 16.0 * (double)p->n;
           const bool plain = p->opts.val_kind == ISPMV_VAL_F64 && p->opts.col_kind == ISPMV_COL_U32;
-          p->opts.variant = !long_rows ? 4 : plain ? 11 : 0;
+          // short rows with scattered columns: the staged per-CTA x windows
+          const bool scattered = p->opts.col_kind == ISPMV_COL_U32 && random_far_fraction(csr) >= 0.05;
+          p->opts.variant = !long_rows ? (scattered ? 26 : 4) : plain ? 11 : 0;
         }
       }
     }
@@ -798,7 +1111,7 @@ cudaTextureObject_t x_texture(ispmv_plan_s *p, const void *src, size_t bytes, bo
   return p->xtex;
 }
 
-template <typename VT, int SPL, int NW, int MINB, bool BUF, bool D16 = false, bool TEX = false>
+template <typename VT, int SPL, int NW, int MINB, bool BUF, bool D16 = false, bool TEX = false, bool STG = false>
 int launch_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, const char *name) {
   if constexpr (sizeof(VT) == 4 && NW == 0) {
     // FP32 values: gather from an FP32 copy of x (the value the FP32 multiply uses)
@@ -821,7 +1134,7 @@ int launch_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, cons
   const cudaTextureObject_t tx = TEX ? x_texture(p, x, (size_t)p->n * 8, false) : 0;
   if (TEX && !tx)
     return launch_wide<VT, SPL, NW, MINB, BUF, D16, false>(p, x, o, s, "stream_wide<tex: x gathered with loads>");
-  auto *k = wide::stream_wide<VT, double, SPL, NW, WIDE_WARPS, MINB, BUF, D16, TEX>;
+  auto *k = wide::stream_wide<VT, double, SPL, NW, WIDE_WARPS, MINB, BUF, D16, TEX, STG>;
   const size_t smem =
       ((NW ? (size_t)p->xw.cap : 0) + (BUF ? (size_t)WIDE_WARPS * 32 * SPL : 0)) * sizeof(double);
   if (smem) ISPMV_TRY(cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -898,6 +1211,15 @@ int run_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
       case 12: return launch_wide_tma<VT, 16, 3, 4>(p, x, o, s, "stream_wide_tma<16,s3,w4>");
       default: return launch_wide_tma<VT, 8, 4, 4>(p, x, o, s, "stream_wide_tma<8,s4,w4>");
     }
+  }
+  if (wc.stg) {
+    if ((reinterpret_cast<uintptr_t>(x) & 15u) == 0) {
+      if (wc.spl == 8) return launch_wide<VT, 8, 1, 4, false, false, false, true>(p, x, o, s, "stream_wide<8,stg,b4>");
+      return launch_wide<VT, 16, 1, 3, false, false, false, true>(p, x, o, s, "stream_wide<16,stg,b3>");
+    }
+    // x not 16-byte aligned (no bulk copy): plain loads over the same stream
+    if (wc.spl == 8) return launch_wide<VT, 8, 0, 4, false>(p, x, o, s, "stream_wide<8,w0,b4,buf0>");
+    return launch_wide<VT, 16, 0, 3, false>(p, x, o, s, "stream_wide<16,w0,b3,buf0>");
   }
   const int nw = wc.win ? std::min(std::max(p->xw.nwin, 0), 3) : 0;
   if (wc.tex) {  // texture gathers (loads where x does not fit a texture)

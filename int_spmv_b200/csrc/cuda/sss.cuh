@@ -386,6 +386,12 @@ struct XWin {
   const UIN *rowmap;   // compressed -> real rows (nullptr: identity)
   UIN n;               // rows (= columns)
   UIN nrows_c;         // compressed rows (non-empty)
+  // per-CTA windows of wide::stream_wide's staged form: CTA b copies
+  // x[tlo[b], tlo[b] + tlen[b]) into shared memory with one bulk copy
+  // (tlo, tlen even; tlo + tlen <= n rounded down to even; tlen <= cap)
+  const UIN *tlo = nullptr;
+  const UIN *tlen = nullptr;
+  int *status = nullptr;  // ISPMV_ERR_TIMEOUT when the copy's wait gave up
 };
 
 struct WinState {

@@ -56,6 +56,14 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
       : "memory");
 }
 
+// The same copy with the default L2 policy (data other CTAs read again).
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(bar))
+               : "memory");
+}
+
 // Prefetches `bytes` (a multiple of 16, 16-byte aligned) of global memory
 // into L2 through the bulk-copy engine; no registers or shared memory.
 __device__ __forceinline__ void prefetch_l2(const void *src, uint32_t bytes) {

@@ -289,7 +289,13 @@ __device__ __forceinline__ void batch(const VT (&v)[SPL], const XT (&xv)[SPL], u
 // TEX: x is gathered with texture fetches (tex1Dfetch on `xtex`, a linear
 // texture over x) instead of global loads: the texture pipe of L1TEX serves
 // the gathers while the load/store pipe streams values and columns.
-template <typename VT, typename XT, int SPL, int NW, int WARPS, int MINB, bool BUF, bool D16 = false, bool TEX = false>
+// STG: one window per CTA chosen by the plan (xw.tlo/xw.tlen: the densest
+// interval of the CTA's columns), copied into shared memory by one bulk copy
+// (cp.async.bulk, no multicast) on an mbarrier, bounded wait; x must be
+// 16-byte aligned (the host checks).  The copy leaves the L1 load pipe to
+// the gathers and costs one copy latency per CTA, not a load loop.
+template <typename VT, typename XT, int SPL, int NW, int WARPS, int MINB, bool BUF, bool D16 = false, bool TEX = false,
+          bool STG = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
     stream_wide(size_t nslots, size_t nslots_pad, size_t seg_slots, size_t nseg, const VT *__restrict__ val,
                 const UIN *__restrict__ col, const UIN *__restrict__ heads, const UIN *__restrict__ segh,
@@ -297,6 +303,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
                 cudaTextureObject_t xtex = 0) {
   static_assert(NW == 0 || sizeof(XT) == 8, "shared-memory x bands hold FP64 x");
   static_assert(!(TEX && NW > 0), "texture gathers replace the shared-memory bands");
+  static_assert(!STG || (NW == 1 && !BUF), "the staged window is one band and uses all dynamic shared memory");
   constexpr int BT = 32 * SPL;
   constexpr unsigned MASK = SPL == 32 ? 0xffffffffu : (1u << SPL) - 1u;
   extern __shared__ __align__(16) double sx[];
@@ -306,7 +313,30 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
   const size_t segid = seg0 + (threadIdx.x >> 5);
   double *rbuf = sx + (NW > 0 ? xw.cap : 0) + (size_t)(threadIdx.x >> 5) * BT;
   Bands<NW> w{};
-  if constexpr (NW > 0) {
+  if constexpr (STG) {
+    __shared__ uint64_t wbar;
+    const UIN lo = __ldg(xw.tlo + blockIdx.x), len = __ldg(xw.tlen + blockIdx.x);
+    if (threadIdx.x == 0 && len) {
+      tma::bar_init(&wbar, 1);
+      tma::fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && len) {
+      tma::bar_expect_tx(&wbar, len * 8u);
+      tma::bulk_g2s(sx, x + lo, len * 8u, &wbar);
+    }
+    const bool ok = !len || tma::bar_wait(&wbar, 0);
+    if (!__syncthreads_and(ok)) {
+      if (threadIdx.x == 0) {
+        if (xw.status) atomicCAS(xw.status, 0, ISPMV_ERR_TIMEOUT);
+        (void)tma::bar_wait(&wbar, 0);  // the copy in flight, before the CTA's shared memory goes
+      }
+      return;
+    }
+    w.lo[0] = lo;
+    w.len[0] = len;
+    w.delta[0] = 0u - lo;
+  } else if constexpr (NW > 0) {
     // the CTA's row range, from the start counts of its first and
     // one-past-last segments, and the bands of x it reads
     if (threadIdx.x == 0) {

@@ -132,6 +132,39 @@ class Plan:
         self.n = csr.n
         self.nnz = csr.nnz
 
+    @classmethod
+    def from_device_csr(cls, row: torch.Tensor, col: torch.Tensor, val: torch.Tensor, *, val_kind="f64",
+                        kernel="auto", variant=0, units_per_warp=0, stream=None) -> "Plan":
+        """The compacted AXT's slot stream built on the GPU from CSR arrays
+        already in device memory (ispmv_plan_dev_csr; u32 arrays as int32
+        tensors): the same arrays as Plan(csr, kernel="wide", variant=...)
+        builds on the host.  Raises IntSpmvError on a malformed CSR."""
+        n, nnz = row.numel() - 1, col.numel()
+        if n < 1 or val.numel() != nnz or val.dtype != torch.float64:
+            raise ValueError("expected row (n+1), col (nnz) and float64 val (nnz) CUDA tensors")
+        o = plan_opts(val_kind, "u32", kernel, units_per_warp, 0, 0.0, variant, 0)
+        h = C.c_void_p()
+        check(load().ispmv_plan_dev_csr(n, nnz, _ptr(row), _ptr(col) if nnz else None, _ptr(val) if nnz else None,
+                                        C.byref(o), C.byref(h), _stream(stream)), "ispmv_plan_dev_csr")
+        self = cls.__new__(cls)
+        self._h, self.n, self.nnz = h, n, nnz
+        return self
+
+    def export_stream(self, stream=None) -> dict:
+        """The slot-stream plan's device arrays as numpy arrays (values as
+        raw bytes), with the layout's lengths."""
+        lib = load()
+        lay = abi.PlanLayout()
+        check(lib.ispmv_plan_get_layout(self._h, C.byref(lay)), "ispmv_plan_get_layout")
+        a = dict(val=np.zeros(lay.slots_pad * lay.val_bytes, np.uint8), col=np.zeros(lay.slots_pad, np.uint32),
+                 heads=np.zeros(lay.slots_pad // 32, np.uint32), segh=np.zeros(lay.nseg, np.uint32),
+                 rowmap=np.zeros(lay.nrowmap, np.uint32), empty=np.zeros(lay.nempty, np.uint32))
+        p = {k: (v.ctypes.data if v.size else None) for k, v in a.items()}
+        check(lib.ispmv_plan_export_stream(self._h, p["val"], p["col"], p["heads"], p["segh"], p["rowmap"],
+                                           p["empty"], _stream(stream)), "ispmv_plan_export_stream")
+        a["layout"] = {f: getattr(lay, f) for f, _ in abi.PlanLayout._fields_}
+        return a
+
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:

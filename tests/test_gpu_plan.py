@@ -21,7 +21,7 @@ COMBOS = [("CSR", "rows"), ("CSR", "ldg"), ("CSR", "tma"), ("AXC", "rows"), ("AX
           ("COM128", "ldg"), ("COM128", "tma"), ("COM256", "ldg"), ("COM512", "tma"),
           ("COM128", "wide"), ("NOC1", "wide"), ("AXC", "wide"), ("CSR", "wide")]
 KIDS = {"ldg": 1, "tma": 2, "rows": 3, "wide": 4}
-WIDE_VARIANTS = list(range(22))
+WIDE_VARIANTS = list(range(31))
 
 
 @pytest.fixture(scope="module")
@@ -351,3 +351,37 @@ def test_wide_texture_gathers_and_fallback(env, val_kind):
         p.spmv(buf[1:])
         p.spmv_graph(xa, yg)
         assert_parity(yg.cpu().numpy(), ref, ab, tol, what=f"tex graph v{variant}")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("val_kind", ["f64", "f32"])
+@pytest.mark.parametrize("variant", [24, 25, 26, 27, 28, 29, 30])
+def test_wide_staged_window(env, val_kind, variant):
+    """Per-CTA x windows copied by one bulk copy: a banded matrix (most
+    columns inside a CTA's window) and a matrix of uniform columns (most
+    outside), n odd (the last x element is never in a window), with an
+    aligned x (the staged kernel) and an x 8 bytes into a buffer (no bulk
+    copy: plain loads over the same stream)."""
+    torch, D, F, orc = env
+    from int_spmv_b200 import matrices as M
+    mats = [M.powerlaw(30001, seed=7, band=300), M.random_csr(20011, 4, rl_max=60, empty_frac=0.05)]
+    tol = TOL_F64 if val_kind == "f64" else TOL_F32
+    for row, col, val in mats:
+        n = len(row) - 1
+        x = M.uniform_x(n, 5)
+        csr = F.CSR(row, col, val)
+        ref, ab = orc.cf_csr(row, col, val, x), orc.abs_csr(row, col, val, x)
+        p = make_plan(F, D, csr, x, "COM128", kernel="wide", variant=variant, val=val_kind)
+        y = p.spmv(torch.from_numpy(x).cuda()).cpu().numpy()
+        assert "stg" in p.kernel_name(), p.kernel_name()
+        assert_parity(y, ref, ab, tol, what=f"staged v{variant}")
+        buf = torch.zeros(n + 1, dtype=torch.float64, device="cuda")
+        buf[1:] = torch.from_numpy(x).cuda()
+        y2 = p.spmv(buf[1:]).cpu().numpy()
+        assert "stg" not in p.kernel_name(), p.kernel_name()
+        assert_parity(y2, ref, ab, tol, what=f"staged fallback v{variant}")
+        yt = torch.from_numpy(np.random.default_rng(3).uniform(-1, 1, n)).cuda()
+        y0 = yt.cpu().numpy()
+        p.spmv(torch.from_numpy(x).cuda(), yt, beta=1)
+        assert_parity(yt.cpu().numpy(), ref + y0, ab + np.abs(y0) * 1e-4, tol, what=f"staged beta1 v{variant}")
+        assert p.status() == 0
