@@ -295,8 +295,9 @@ typedef struct ispmv_plan_s *ispmv_plan;
 #define ISPMV_KERNEL_TMA 2   /* slot-stream kernel, 1D bulk copies (cp.async.bulk) into shared memory */
 #define ISPMV_KERNEL_ROWS 3  /* row-parallel kernel (CSR: lanes per row; AXC: 8 lanes per row; K1) */
 #define ISPMV_KERNEL_WIDE 4  /* slot-stream kernel over a lane-interleaved copy of the stream: 16 (or 8)
-                                slots per lane, diagonal x bands in shared memory (FP64/FP32 values,
-                                u32 columns; SpMV only) */
+                                slots per lane; variants with diagonal x bands or a per-CTA x window
+                                in shared memory (FP64/FP32 values, u32 columns), and plain-load
+                                variants that also take 16-bit column deltas and BF16 lo-words */
 #define ISPMV_VARIANT_QUEUE 16 /* slot-stream kernel as a work queue drained by persistent warps */
 
 typedef struct {
@@ -306,7 +307,7 @@ typedef struct {
   int ctas_per_sm;   /* 0 = library default */
   int units_per_warp;/* work granule of one warp; 0 = library default */
   double lo_tol;     /* F32_LO16: rows whose FP32 rounding error bound exceeds
-                        lo_tol relative carry a lo-word; 0 = default 1e-9 */
+                        lo_tol relative carry a lo-word; 0 = default 1e-6 */
   int variant;       /* kernel variant (prefetch depth / register budget); 0 = default;
                         ISPMV_VARIANT_QUEUE = persistent warps pulling segments
                         from a device work queue */

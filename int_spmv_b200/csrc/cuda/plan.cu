@@ -431,10 +431,11 @@ int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v,
   const bool wide = p->opts.kernel == ISPMV_KERNEL_WIDE;
   if (wide) {
     const WideCfg wc = wide_variant(p->opts.variant);
-    if (p->opts.val_kind == ISPMV_VAL_F32_LO16 ||
-        (p->opts.col_kind == ISPMV_COL_D16 && (wc.win || wc.tma || wc.buf || wc.tmem || wc.stg)))
+    const bool lo16 = p->opts.val_kind == ISPMV_VAL_F32_LO16;
+    if ((narrow_kinds(p) && (wc.win || wc.tma || wc.buf || wc.tmem || wc.stg)) || (lo16 && wc.tex))
       return fail(ISPMV_ERR_UNSUPPORTED,
-                  "stream_wide: FP64/FP32 values; 16-bit column deltas on the plain-load variants without x bands");
+                  "stream_wide: 16-bit column deltas and BF16 lo-words on the plain-load variants without x bands "
+                  "(lo-words: not the texture-gather variants)");
     xc = {wc.warps, wc.cap, wc.seg};
     xwv = wc.win;
   }
@@ -567,13 +568,20 @@ int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v,
       const size_t a = start[r], e = start[r] + (csr->row[r + 1] - csr->row[r]);
       for (size_t sg = a / p->seg_slots; sg <= (e - 1) / p->seg_slots && sg < p->nseg; sg++) segflag[sg] = 1;
     }
+    // a flagged segment's residuals in slot order, or lane-interleaved like
+    // the 16-bit deltas (8 per vector) for the lane-interleaved kernel; its
+    // slot count is a multiple of the batch, so batches stay whole
+    const unsigned ilspl = wide ? (unsigned)wide_variant(p->opts.variant).spl : 0u;
     std::vector<UIN> off(p->nseg, NO_ROW);
     std::vector<uint16_t> lo;
     for (size_t sg = 0; sg < p->nseg; sg++) {
       if (!segflag[sg]) continue;
-      off[sg] = (UIN)lo.size();
+      const size_t base = lo.size();
+      off[sg] = (UIN)base;
       const size_t a = sg * p->seg_slots, e = std::min(p->slots_pad, a + p->seg_slots);
-      for (size_t q = a; q < e; q++) lo.push_back(to_bf16((float)(v[q] - (double)(float)v[q])));
+      lo.resize(base + (e - a));
+      for (size_t q = a; q < e; q++)
+        lo[base + (ilspl ? wide::il_pos(q - a, ilspl, 8u) : q - a)] = to_bf16((float)(v[q] - (double)(float)v[q]));
     }
     p->lo_frac = p->slots ? (double)lo.size() / (double)p->slots_pad : 0.0;
     uint16_t *dl; UIN *dof;
@@ -983,21 +991,18 @@ ISPMV_API int ispmv_plan_axt(const str_matCSR *csr, const str_matAXT *axt, const
     std::vector<size_t> start(p->n);
     for (UIN r = 0; r < p->n; r++) start[r] = (size_t)(axt->con[r] / 16) * 8 + axt->con[r] % 16;
     if (p->opts.kernel == ISPMV_KERNEL_AUTO) {
-      // the lane-interleaved kernel where it takes the value/column forms:
-      // 8 slots per lane for rows of fewer than 16 slots on average; else 16,
-      // bulk-copy staged for FP64 values with u32 columns (measured fastest
-      // there), plain loads for the FP32 and 16-bit-delta forms
-      if (p->opts.val_kind == ISPMV_VAL_F32_LO16) {
-        p->opts.kernel = ISPMV_KERNEL_LDG;
-      } else {
-        p->opts.kernel = ISPMV_KERNEL_WIDE;
-        if (p->opts.variant == 0) {
-          const bool long_rows = (double)p->slots >= 16.0 * (double)p->n;
-          const bool plain = p->opts.val_kind == ISPMV_VAL_F64 && p->opts.col_kind == ISPMV_COL_U32;
-          // short rows with scattered columns: the staged per-CTA x windows
-          const bool scattered = p->opts.col_kind == ISPMV_COL_U32 && random_far_fraction(csr) >= 0.05;
-          p->opts.variant = !long_rows ? (scattered ? 26 : 4) : plain ? 11 : 0;
-        }
+      // the lane-interleaved kernel: 8 slots per lane for rows of fewer than
+      // 16 slots on average (with per-CTA x windows where the columns are
+      // scattered); else 16, bulk-copy staged for FP64 values with u32
+      // columns (measured fastest there), plain loads for the FP32, lo-word
+      // and 16-bit-delta forms
+      p->opts.kernel = ISPMV_KERNEL_WIDE;
+      if (p->opts.variant == 0) {
+        const bool long_rows = (double)p->slots >= 16.0 * (double)p->n;
+        const bool plain = p->opts.val_kind == ISPMV_VAL_F64 && p->opts.col_kind == ISPMV_COL_U32;
+        // short rows with scattered columns: the staged per-CTA x windows
+        const bool scattered = !narrow_kinds(p) && random_far_fraction(csr) >= 0.05;
+        p->opts.variant = !long_rows ? (scattered ? 26 : 4) : plain ? 11 : 0;
       }
     }
     st = setup_stream(p, csr, v, c, start);
@@ -1111,9 +1116,10 @@ cudaTextureObject_t x_texture(ispmv_plan_s *p, const void *src, size_t bytes, bo
   return p->xtex;
 }
 
-template <typename VT, int SPL, int NW, int MINB, bool BUF, bool D16 = false, bool TEX = false, bool STG = false>
+template <typename VT, int SPL, int NW, int MINB, bool BUF, bool D16 = false, bool TEX = false, bool STG = false,
+          bool LO = false>
 int launch_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, const char *name) {
-  if constexpr (sizeof(VT) == 4 && NW == 0) {
+  if constexpr (sizeof(VT) == 4 && NW == 0 && !LO) {
     // FP32 values: gather from an FP32 copy of x (the value the FP32 multiply uses)
     if (!p->x32) TRY(dev_alloc(p, p->n, &p->x32));
     const unsigned gc = (unsigned)std::min<size_t>(((size_t)p->n / 2 + 255) / 256, (size_t)sm_count() * 8) + 1;
@@ -1134,7 +1140,7 @@ int launch_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, cons
   const cudaTextureObject_t tx = TEX ? x_texture(p, x, (size_t)p->n * 8, false) : 0;
   if (TEX && !tx)
     return launch_wide<VT, SPL, NW, MINB, BUF, D16, false>(p, x, o, s, "stream_wide<tex: x gathered with loads>");
-  auto *k = wide::stream_wide<VT, double, SPL, NW, WIDE_WARPS, MINB, BUF, D16, TEX, STG>;
+  auto *k = wide::stream_wide<VT, double, SPL, NW, WIDE_WARPS, MINB, BUF, D16, TEX, STG, LO>;
   const size_t smem =
       ((NW ? (size_t)p->xw.cap : 0) + (BUF ? (size_t)WIDE_WARPS * 32 * SPL : 0)) * sizeof(double);
   if (smem) ISPMV_TRY(cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1210,6 +1216,19 @@ int run_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
       case 11: return launch_wide_tma<VT, 16, 2, 4>(p, x, o, s, "stream_wide_tma<16,s2,w4>");
       case 12: return launch_wide_tma<VT, 16, 3, 4>(p, x, o, s, "stream_wide_tma<16,s3,w4>");
       default: return launch_wide_tma<VT, 8, 4, 4>(p, x, o, s, "stream_wide_tma<8,s4,w4>");
+    }
+  }
+  if constexpr (sizeof(VT) == 4) {
+    if (p->opts.val_kind == ISPMV_VAL_F32_LO16) {  // plain loads, FP64 x, no bands (setup checks)
+      const bool d = p->opts.col_kind == ISPMV_COL_D16;
+      if (wc.spl == 8)
+        return d ? launch_wide<VT, 8, 0, 4, false, true, false, false, true>(p, x, o, s, "stream_wide<8,w0,b4,buf0,d16,lo>")
+                 : launch_wide<VT, 8, 0, 4, false, false, false, false, true>(p, x, o, s, "stream_wide<8,w0,b4,buf0,lo>");
+      if (wc.minb == 2)
+        return d ? launch_wide<VT, 16, 0, 2, false, true, false, false, true>(p, x, o, s, "stream_wide<16,w0,b2,buf0,d16,lo>")
+                 : launch_wide<VT, 16, 0, 2, false, false, false, false, true>(p, x, o, s, "stream_wide<16,w0,b2,buf0,lo>");
+      return d ? launch_wide<VT, 16, 0, 3, false, true, false, false, true>(p, x, o, s, "stream_wide<16,w0,b3,buf0,d16,lo>")
+               : launch_wide<VT, 16, 0, 3, false, false, false, false, true>(p, x, o, s, "stream_wide<16,w0,b3,buf0,lo>");
     }
   }
   if (wc.stg) {

@@ -294,8 +294,12 @@ __device__ __forceinline__ void batch(const VT (&v)[SPL], const XT (&xv)[SPL], u
 // (cp.async.bulk, no multicast) on an mbarrier, bounded wait; x must be
 // 16-byte aligned (the host checks).  The copy leaves the L1 load pipe to
 // the gathers and costs one copy latency per CTA, not a load loop.
+// LO (FP32 values, FP64 x): in segments whose rows need it, a BF16 residual
+// per slot (nw.lo16 at nw.lo_off[segment], lane-interleaved like D16's
+// deltas); such a segment multiplies hi + lo (exact in FP64 unless lo is
+// below 2^-45 of hi) by x in FP64, the others multiply in FP32.
 template <typename VT, typename XT, int SPL, int NW, int WARPS, int MINB, bool BUF, bool D16 = false, bool TEX = false,
-          bool STG = false>
+          bool STG = false, bool LO = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
     stream_wide(size_t nslots, size_t nslots_pad, size_t seg_slots, size_t nseg, const VT *__restrict__ val,
                 const UIN *__restrict__ col, const UIN *__restrict__ heads, const UIN *__restrict__ segh,
@@ -304,6 +308,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
   static_assert(NW == 0 || sizeof(XT) == 8, "shared-memory x bands hold FP64 x");
   static_assert(!(TEX && NW > 0), "texture gathers replace the shared-memory bands");
   static_assert(!STG || (NW == 1 && !BUF), "the staged window is one band and uses all dynamic shared memory");
+  static_assert(!LO || (sizeof(VT) == 4 && sizeof(XT) == 8), "lo-words correct FP32 values against FP64 x");
   constexpr int BT = 32 * SPL;
   constexpr unsigned MASK = SPL == 32 ? 0xffffffffu : (1u << SPL) - 1u;
   extern __shared__ __align__(16) double sx[];
@@ -381,6 +386,8 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
   const int nbat = (int)((s1 - s0) / BT);
   sss::Run st;
   sss::begin(st, o, segid, segh[segid], __ldg(heads + (s0 >> 5)));
+  UIN lo_base = NO_ROW;
+  if constexpr (LO) lo_base = __ldg(nw.lo_off + segid);
   for (int j = 0; j < nbat; j++) {
     const size_t b = s0 + (size_t)j * BT;
     Vals<VT, SPL> v;
@@ -430,6 +437,17 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
 #pragma unroll
       for (int k = 0; k < SPL; k++)
         if (sl + k >= nslots) xv[k] = (XT)0;
+    }
+    if constexpr (LO) {
+      if (lo_base != NO_ROW) {  // the segment's residuals: FP64 values hi + lo
+        Deltas<SPL> lw;
+        lw.get(nw.lo16 + lo_base, b - s0, lane);
+        double vd[SPL];
+#pragma unroll
+        for (int k = 0; k < SPL; k++) vd[k] = (double)vv[k] + sss::bf16_to_double((uint16_t)lw[k]);
+        batch<double, XT, SPL, BUF>(vd, xv, bits, st, o, rbuf);
+        continue;
+      }
     }
     batch<VT, XT, SPL, BUF>(vv, xv, bits, st, o, rbuf);
   }

@@ -149,7 +149,9 @@ def test_wide_rejects_other_forms(env):
     with pytest.raises(IntSpmvError):
         make_plan(F, D, csr, g["x"], "COM128", col="d16", kernel="wide", variant=1)  # row buffer: u32 columns only
     with pytest.raises(IntSpmvError):
-        make_plan(F, D, csr, g["x"], "COM128", val="f32lo", kernel="wide")
+        make_plan(F, D, csr, g["x"], "COM128", val="f32lo", kernel="wide", variant=2)  # x bands: no lo-words
+    with pytest.raises(IntSpmvError):
+        make_plan(F, D, csr, g["x"], "COM128", val="f32lo", kernel="wide", variant=16)  # texture gathers: no lo-words
 
 
 WIDE_D16 = [0, 4, 8, 9, 14, 15, 16, 17]
@@ -172,11 +174,38 @@ def test_wide_d16(env, fmt, variant, val_kind):
             assert p.info["kernel"] == 4 and p.info["col_kind"] == 1 and "d16" in p.kernel_name()
 
 
+WIDE_LO = [0, 4, 8, 9, 14, 15]
+
+
+@pytest.mark.parametrize("fmt", ["COM128", "NOC1", "CSR"])
+@pytest.mark.parametrize("variant", WIDE_LO)
+@pytest.mark.parametrize("col_kind", ["u32", "d16"])
+def test_wide_lo(env, fmt, variant, col_kind):
+    """BF16 lo-words on the lane-interleaved kernel (FP32 values, FP64 x):
+    the default tolerance (flagged segments only) and every row flagged
+    (hi + lo within 1e-8), on banded, stencil, random and long-row matrices."""
+    torch, D, F, orc = env
+    from int_spmv_b200 import matrices as M
+    mats = [M.fem_banded(20011, np.random.default_rng(5), 3, 30), M.stencil27(22, seed=2),
+            M.random_csr(7001, 12, rl_max=90, empty_frac=0.1), M.random_csr(3001, 9, rl_max=700, empty_frac=0.2)]
+    for i, (row, col, val) in enumerate(mats):
+        x = M.uniform_x(len(row) - 1, 40 + i)
+        for beta in (0, 1):
+            p, _ = check_plan(env, row, col, val, x, fmt, "f32lo", beta, kernel="wide", variant=variant, col=col_kind)
+            assert p.info["kernel"] == 4 and p.kernel_name().endswith("lo>")
+        csr = F.CSR(row, col, val)
+        p = make_plan(F, D, csr, x, fmt, val="f32lo", kernel="wide", variant=variant, col=col_kind, lo_tol=1e-300)
+        y = p.spmv(torch.from_numpy(x).cuda()).cpu().numpy()
+        assert_parity(y, orc.cf_csr(row, col, val, x), orc.abs_csr(row, col, val, x), 1e-8,
+                      what=f"{fmt} wide v{variant} f32lo all rows")
+
+
 @pytest.mark.parametrize("fmt", ["COM128", "NOC1"])
 def test_auto_picks_wide(env, fmt):
     """AXT COM and tileH=1 plans default to the lane-interleaved kernel: 16
-    slots per lane for long rows, 8 for short, u32 or 16-bit columns; the
-    BF16 lo-word form keeps stream_ldg."""
+    slots per lane for long rows, 8 for short (with per-CTA x windows: the
+    columns are uniformly scattered), u32 or 16-bit columns, and the BF16
+    lo-word form."""
     torch, D, F, orc = env
     from int_spmv_b200 import matrices as M
     for rl_max, name in ((8, "stream_wide<8,"), (60, "stream_wide_tma<16,")):
@@ -190,7 +219,7 @@ def test_auto_picks_wide(env, fmt):
         p, _ = check_plan(env, row, col, val, x, fmt, col="d16")
         assert p.info["kernel"] == 4 and p.kernel_name().endswith("d16>")
         p, _ = check_plan(env, row, col, val, x, fmt, val_kind="f32lo")
-        assert p.info["kernel"] == 1
+        assert p.info["kernel"] == 4 and p.kernel_name().endswith("lo>")
 
 
 @pytest.mark.parametrize("fmt,kernel", [("NOC1", "ldg"), ("NOC4", "tma"), ("COM128", "ldg"), ("COM128", "tma"),
