@@ -245,6 +245,7 @@ struct WideCfg {
   bool tmem = false;  // stream staged through tensor memory (stream_tmem); stages = TMEM stages,
                       // warps = consumer warps per CTA (4 per column half)
   bool stg = false;   // one x window per CTA (cap doubles), chosen at plan time, copied by one bulk copy
+  bool pfc = false;   // the next batch's columns loaded one batch ahead
 };
 constexpr int WIDE_WARPS = 8;
 WideCfg wide_variant(int v) {
@@ -283,6 +284,12 @@ WideCfg wide_variant(int v) {
     case 28: return {8, false, 2048, 512, 4, false, false, 0, 8, false, false, true};
     case 29: return {8, false, 3072, 512, 4, false, false, 0, 8, false, false, true};
     case 30: return {8, false, 2560, 1024, 4, false, false, 0, 8, false, false, true};
+    // the next batch's columns loaded one batch ahead, with and without the
+    // per-CTA x window, at 4 and 3 CTAs per SM
+    case 31: return {8, false, 3072, 1024, 4, false, false, 0, 8, false, false, true, true};
+    case 32: return {8, false, 0, 2048, 4, false, false, 0, 8, false, false, false, true};
+    case 33: return {8, false, 0, 2048, 3, false, false, 0, 8, false, false, false, true};
+    case 34: return {8, false, 3072, 1024, 3, false, false, 0, 8, false, false, true, true};
     default: return {16, false, 0, 4096, 3, false, false, 0, 8};
   }
 }
@@ -432,7 +439,7 @@ int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v,
   if (wide) {
     const WideCfg wc = wide_variant(p->opts.variant);
     const bool lo16 = p->opts.val_kind == ISPMV_VAL_F32_LO16;
-    if ((narrow_kinds(p) && (wc.win || wc.tma || wc.buf || wc.tmem || wc.stg)) || (lo16 && wc.tex))
+    if ((narrow_kinds(p) && (wc.win || wc.tma || wc.buf || wc.tmem || wc.stg || wc.pfc)) || (lo16 && wc.tex))
       return fail(ISPMV_ERR_UNSUPPORTED,
                   "stream_wide: 16-bit column deltas and BF16 lo-words on the plain-load variants without x bands "
                   "(lo-words: not the texture-gather variants)");
@@ -992,17 +999,16 @@ ISPMV_API int ispmv_plan_axt(const str_matCSR *csr, const str_matAXT *axt, const
     for (UIN r = 0; r < p->n; r++) start[r] = (size_t)(axt->con[r] / 16) * 8 + axt->con[r] % 16;
     if (p->opts.kernel == ISPMV_KERNEL_AUTO) {
       // the lane-interleaved kernel: 8 slots per lane for rows of fewer than
-      // 16 slots on average (with per-CTA x windows where the columns are
+      // 16 nonzeros on average (with per-CTA x windows where the columns are
       // scattered); else 16, bulk-copy staged for FP64 values with u32
-      // columns (measured fastest there), plain loads for the FP32, lo-word
-      // and 16-bit-delta forms
+      // columns that are not scattered (measured fastest there), plain loads
+      // for scattered columns and for the FP32, lo-word and 16-bit-delta forms
       p->opts.kernel = ISPMV_KERNEL_WIDE;
       if (p->opts.variant == 0) {
-        const bool long_rows = (double)p->slots >= 16.0 * (double)p->n;
+        const bool long_rows = (double)csr->nnz >= 16.0 * (double)p->n;
         const bool plain = p->opts.val_kind == ISPMV_VAL_F64 && p->opts.col_kind == ISPMV_COL_U32;
-        // short rows with scattered columns: the staged per-CTA x windows
-        const bool scattered = !narrow_kinds(p) && random_far_fraction(csr) >= 0.05;
-        p->opts.variant = !long_rows ? (scattered ? 26 : 4) : plain ? 11 : 0;
+        const bool scattered = random_far_fraction(csr) >= 0.05;
+        p->opts.variant = !long_rows ? (scattered && !narrow_kinds(p) ? 26 : 4) : plain && !scattered ? 11 : 0;
       }
     }
     st = setup_stream(p, csr, v, c, start);
@@ -1117,7 +1123,7 @@ cudaTextureObject_t x_texture(ispmv_plan_s *p, const void *src, size_t bytes, bo
 }
 
 template <typename VT, int SPL, int NW, int MINB, bool BUF, bool D16 = false, bool TEX = false, bool STG = false,
-          bool LO = false>
+          bool LO = false, bool PFC = false>
 int launch_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, const char *name) {
   if constexpr (sizeof(VT) == 4 && NW == 0 && !LO) {
     // FP32 values: gather from an FP32 copy of x (the value the FP32 multiply uses)
@@ -1129,7 +1135,7 @@ int launch_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, cons
     const cudaTextureObject_t tx = TEX ? x_texture(p, p->x32, (size_t)p->n * 4, true) : 0;
     if (TEX && !tx)
       return launch_wide<VT, SPL, NW, MINB, BUF, D16, false>(p, x, o, s, "stream_wide<tex: x gathered with loads>");
-    auto *k = wide::stream_wide<VT, float, SPL, NW, WIDE_WARPS, MINB, BUF, D16, TEX>;
+    auto *k = wide::stream_wide<VT, float, SPL, NW, WIDE_WARPS, MINB, BUF, D16, TEX, false, false, PFC>;
     const size_t smem = (BUF ? (size_t)WIDE_WARPS * 32 * SPL : 0) * sizeof(double);
     if (smem) ISPMV_TRY(cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k<<<(unsigned)((p->nseg + WIDE_WARPS - 1) / WIDE_WARPS), WIDE_WARPS * 32, smem, s>>>(
@@ -1140,7 +1146,7 @@ int launch_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, cons
   const cudaTextureObject_t tx = TEX ? x_texture(p, x, (size_t)p->n * 8, false) : 0;
   if (TEX && !tx)
     return launch_wide<VT, SPL, NW, MINB, BUF, D16, false>(p, x, o, s, "stream_wide<tex: x gathered with loads>");
-  auto *k = wide::stream_wide<VT, double, SPL, NW, WIDE_WARPS, MINB, BUF, D16, TEX, STG, LO>;
+  auto *k = wide::stream_wide<VT, double, SPL, NW, WIDE_WARPS, MINB, BUF, D16, TEX, STG, LO, PFC>;
   const size_t smem =
       ((NW ? (size_t)p->xw.cap : 0) + (BUF ? (size_t)WIDE_WARPS * 32 * SPL : 0)) * sizeof(double);
   if (smem) ISPMV_TRY(cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -1230,6 +1236,14 @@ int run_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
       return d ? launch_wide<VT, 16, 0, 3, false, true, false, false, true>(p, x, o, s, "stream_wide<16,w0,b3,buf0,d16,lo>")
                : launch_wide<VT, 16, 0, 3, false, false, false, false, true>(p, x, o, s, "stream_wide<16,w0,b3,buf0,lo>");
     }
+  }
+  if (wc.pfc) {  // u32 columns (setup checks); the window where x allows the bulk copy
+    const bool win = wc.stg && (reinterpret_cast<uintptr_t>(x) & 15u) == 0;
+    if (wc.minb == 3)
+      return win ? launch_wide<VT, 8, 1, 3, false, false, false, true, false, true>(p, x, o, s, "stream_wide<8,stg,b3,pfc>")
+                 : launch_wide<VT, 8, 0, 3, false, false, false, false, false, true>(p, x, o, s, "stream_wide<8,w0,b3,pfc>");
+    return win ? launch_wide<VT, 8, 1, 4, false, false, false, true, false, true>(p, x, o, s, "stream_wide<8,stg,b4,pfc>")
+               : launch_wide<VT, 8, 0, 4, false, false, false, false, false, true>(p, x, o, s, "stream_wide<8,w0,b4,pfc>");
   }
   if (wc.stg) {
     if ((reinterpret_cast<uintptr_t>(x) & 15u) == 0) {

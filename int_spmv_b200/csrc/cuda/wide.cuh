@@ -298,8 +298,10 @@ __device__ __forceinline__ void batch(const VT (&v)[SPL], const XT (&xv)[SPL], u
 // per slot (nw.lo16 at nw.lo_off[segment], lane-interleaved like D16's
 // deltas); such a segment multiplies hi + lo (exact in FP64 unless lo is
 // below 2^-45 of hi) by x in FP64, the others multiply in FP32.
+// PFC: the next batch's columns are loaded one batch ahead (u32 columns),
+// so a batch's gathers issue without waiting for its column load.
 template <typename VT, typename XT, int SPL, int NW, int WARPS, int MINB, bool BUF, bool D16 = false, bool TEX = false,
-          bool STG = false, bool LO = false>
+          bool STG = false, bool LO = false, bool PFC = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
     stream_wide(size_t nslots, size_t nslots_pad, size_t seg_slots, size_t nseg, const VT *__restrict__ val,
                 const UIN *__restrict__ col, const UIN *__restrict__ heads, const UIN *__restrict__ segh,
@@ -309,6 +311,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
   static_assert(!(TEX && NW > 0), "texture gathers replace the shared-memory bands");
   static_assert(!STG || (NW == 1 && !BUF), "the staged window is one band and uses all dynamic shared memory");
   static_assert(!LO || (sizeof(VT) == 4 && sizeof(XT) == 8), "lo-words correct FP32 values against FP64 x");
+  static_assert(!(PFC && D16), "column prefetch reads u32 columns");
   constexpr int BT = 32 * SPL;
   constexpr unsigned MASK = SPL == 32 ? 0xffffffffu : (1u << SPL) - 1u;
   extern __shared__ __align__(16) double sx[];
@@ -388,6 +391,10 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
   sss::begin(st, o, segid, segh[segid], __ldg(heads + (s0 >> 5)));
   UIN lo_base = NO_ROW;
   if constexpr (LO) lo_base = __ldg(nw.lo_off + segid);
+  Cols<SPL> cnext;  // PFC: the columns of batch j + 1
+  if constexpr (PFC) {
+    if (nbat > 0) cnext.get(col, s0, lane);
+  }
   for (int j = 0; j < nbat; j++) {
     const size_t b = s0 + (size_t)j * BT;
     Vals<VT, SPL> v;
@@ -406,6 +413,10 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
 #pragma unroll
         for (int k = 0; k < SPL; k++) c[k] = m + d[k];
       }
+    } else if constexpr (PFC) {
+#pragma unroll
+      for (int k = 0; k < SPL; k++) c[k] = cnext[k];
+      if (j + 1 < nbat) cnext.get(col, b + BT, lane);
     } else {
       Cols<SPL> e;
       e.get(col, b, lane);

@@ -21,7 +21,7 @@ COMBOS = [("CSR", "rows"), ("CSR", "ldg"), ("CSR", "tma"), ("AXC", "rows"), ("AX
           ("COM128", "ldg"), ("COM128", "tma"), ("COM256", "ldg"), ("COM512", "tma"),
           ("COM128", "wide"), ("NOC1", "wide"), ("AXC", "wide"), ("CSR", "wide")]
 KIDS = {"ldg": 1, "tma": 2, "rows": 3, "wide": 4}
-WIDE_VARIANTS = list(range(31))
+WIDE_VARIANTS = list(range(35))
 
 
 @pytest.fixture(scope="module")
@@ -203,16 +203,17 @@ def test_wide_lo(env, fmt, variant, col_kind):
 @pytest.mark.parametrize("fmt", ["COM128", "NOC1"])
 def test_auto_picks_wide(env, fmt):
     """AXT COM and tileH=1 plans default to the lane-interleaved kernel: 16
-    slots per lane for long rows, 8 for short (with per-CTA x windows: the
-    columns are uniformly scattered), u32 or 16-bit columns, and the BF16
-    lo-word form."""
+    slots per lane for rows of 16+ nonzeros (bulk-copy staged unless the
+    columns are scattered), 8 for short rows (with per-CTA x windows where
+    the columns are uniformly scattered, not on fixed far diagonals), u32 or
+    16-bit columns, and the BF16 lo-word form."""
     torch, D, F, orc = env
     from int_spmv_b200 import matrices as M
-    for rl_max, name in ((8, "stream_wide<8,"), (60, "stream_wide_tma<16,")):
+    for rl_max, name in ((8, "stream_wide<8,stg"), (60, "stream_wide<16,")):
         row, col, val = M.random_csr(5000, rl_max, rl_max=rl_max, empty_frac=0.05)
         x = M.uniform_x(5000, rl_max)
         p, _ = check_plan(env, row, col, val, x, fmt)
-        assert p.info["kernel"] == 4 and p.kernel_name().startswith(name)
+        assert p.info["kernel"] == 4 and p.kernel_name().startswith(name), p.kernel_name()
         if rl_max > 8:
             p, _ = check_plan(env, row, col, val, x, fmt, val_kind="f32")
             assert p.kernel_name().startswith("stream_wide<16,")
@@ -220,6 +221,21 @@ def test_auto_picks_wide(env, fmt):
         assert p.info["kernel"] == 4 and p.kernel_name().endswith("d16>")
         p, _ = check_plan(env, row, col, val, x, fmt, val_kind="f32lo")
         assert p.info["kernel"] == 4 and p.kernel_name().endswith("lo>")
+    # short rows whose far columns sit on fixed diagonals (+-1700): neighbouring
+    # rows share lines, so no per-CTA window
+    n = 20000
+    r = np.repeat(np.arange(n), 3)
+    c = (r + np.tile([-1700, 0, 1700], n)) % n
+    order = np.lexsort((c, r))
+    row = np.arange(0, 3 * n + 1, 3, dtype=np.uint32)
+    col, val = c[order].astype(np.uint32), np.random.default_rng(2).normal(size=3 * n)
+    p, _ = check_plan(env, row, col, val, M.uniform_x(n, 2), fmt)
+    assert p.kernel_name().startswith("stream_wide<8,w0"), p.kernel_name()
+    # long rows whose columns are not scattered (27-point stencil): the
+    # bulk-copy staged stream
+    row, col, val = M.stencil27(20, seed=2)
+    p, _ = check_plan(env, row, col, val, M.uniform_x(8000, 2), fmt)
+    assert p.kernel_name().startswith("stream_wide_tma<16,"), p.kernel_name()
 
 
 @pytest.mark.parametrize("fmt,kernel", [("NOC1", "ldg"), ("NOC4", "tma"), ("COM128", "ldg"), ("COM128", "tma"),
@@ -384,7 +400,7 @@ def test_wide_texture_gathers_and_fallback(env, val_kind):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("val_kind", ["f64", "f32"])
-@pytest.mark.parametrize("variant", [24, 25, 26, 27, 28, 29, 30])
+@pytest.mark.parametrize("variant", [24, 25, 26, 27, 28, 29, 30, 31, 34])
 def test_wide_staged_window(env, val_kind, variant):
     """Per-CTA x windows copied by one bulk copy: a banded matrix (most
     columns inside a CTA's window) and a matrix of uniform columns (most
