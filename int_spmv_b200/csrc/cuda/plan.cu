@@ -999,16 +999,20 @@ ISPMV_API int ispmv_plan_axt(const str_matCSR *csr, const str_matAXT *axt, const
     for (UIN r = 0; r < p->n; r++) start[r] = (size_t)(axt->con[r] / 16) * 8 + axt->con[r] % 16;
     if (p->opts.kernel == ISPMV_KERNEL_AUTO) {
       // the lane-interleaved kernel: 8 slots per lane for rows of fewer than
-      // 16 nonzeros on average (with per-CTA x windows where the columns are
-      // scattered); else 16, bulk-copy staged for FP64 values with u32
-      // columns that are not scattered (measured fastest there), plain loads
-      // for scattered columns and for the FP32, lo-word and 16-bit-delta forms
+      // 16 nonzeros on average, where the columns are scattered with per-CTA
+      // x windows (FP64 values) or the next batch's columns loaded ahead
+      // (FP32 values, whose kernel has the registers for it); else 16,
+      // bulk-copy staged for FP64 values with u32 columns that are not
+      // scattered (measured fastest there), plain loads for scattered columns
+      // and for the FP32, lo-word and 16-bit-delta forms
       p->opts.kernel = ISPMV_KERNEL_WIDE;
       if (p->opts.variant == 0) {
         const bool long_rows = (double)csr->nnz >= 16.0 * (double)p->n;
         const bool plain = p->opts.val_kind == ISPMV_VAL_F64 && p->opts.col_kind == ISPMV_COL_U32;
         const bool scattered = random_far_fraction(csr) >= 0.05;
-        p->opts.variant = !long_rows ? (scattered && !narrow_kinds(p) ? 26 : 4) : plain && !scattered ? 11 : 0;
+        const int short_scattered = p->opts.val_kind == ISPMV_VAL_F32 ? 32 : 26;
+        p->opts.variant = !long_rows ? (scattered && !narrow_kinds(p) ? short_scattered : 4)
+                                     : plain && !scattered ? 11 : 0;
       }
     }
     st = setup_stream(p, csr, v, c, start);

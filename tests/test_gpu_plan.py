@@ -204,9 +204,10 @@ def test_wide_lo(env, fmt, variant, col_kind):
 def test_auto_picks_wide(env, fmt):
     """AXT COM and tileH=1 plans default to the lane-interleaved kernel: 16
     slots per lane for rows of 16+ nonzeros (bulk-copy staged unless the
-    columns are scattered), 8 for short rows (with per-CTA x windows where
-    the columns are uniformly scattered, not on fixed far diagonals), u32 or
-    16-bit columns, and the BF16 lo-word form."""
+    columns are scattered), 8 for short rows (where the columns are uniformly
+    scattered, not on fixed far diagonals: per-CTA x windows for FP64 values,
+    column prefetch for FP32 values), u32 or 16-bit columns, and the BF16
+    lo-word form."""
     torch, D, F, orc = env
     from int_spmv_b200 import matrices as M
     for rl_max, name in ((8, "stream_wide<8,stg"), (60, "stream_wide<16,")):
@@ -214,6 +215,9 @@ def test_auto_picks_wide(env, fmt):
         x = M.uniform_x(5000, rl_max)
         p, _ = check_plan(env, row, col, val, x, fmt)
         assert p.info["kernel"] == 4 and p.kernel_name().startswith(name), p.kernel_name()
+        if rl_max == 8:  # FP32 values, scattered short rows: the next batch's columns loaded ahead
+            p, _ = check_plan(env, row, col, val, x, fmt, val_kind="f32")
+            assert p.kernel_name().startswith("stream_wide<8,w0,b4,pfc>"), p.kernel_name()
         if rl_max > 8:
             p, _ = check_plan(env, row, col, val, x, fmt, val_kind="f32")
             assert p.kernel_name().startswith("stream_wide<16,")
