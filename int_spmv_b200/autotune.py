@@ -40,6 +40,7 @@ SPMV_CANDIDATES = [
     ("COM128", dict(kernel="wide", variant=7)),   # 8 slots per lane, shared-memory x band
     ("COM128", dict(kernel="wide", variant=16)),  # 8 slots per lane, x gathered through the texture pipe
     ("COM128", dict(kernel="wide", variant=26)),  # 8 slots per lane, per-CTA x window by one bulk copy
+    ("COM128", dict(kernel="wide", variant=32)),  # 8 slots per lane, next batch's columns loaded ahead
     ("NOC1", dict(kernel="wide", variant=0)),
     ("COM128", dict(kernel="ldg", variant=0)),
     ("COM128", dict(kernel="ldg", variant=2)),
