@@ -334,10 +334,10 @@ int ispmv_plan_destroy(ispmv_plan p);
  * conversion (getFormatDataAXT, intSpmv_main.c:1275-1381) for the compacted
  * AXT's slot stream (CSR order).  The arrays are bit for bit those
  * ispmv_plan_csr builds for the same matrix with kernel ISPMV_KERNEL_WIDE and
- * the same variant.  d_row (n+1), d_col and d_val (nnz) are device pointers,
- * read during the call.  Options: val_kind F64 or F32, col_kind U32, kernel
- * AUTO (the compacted AXT's default variant) or WIDE with a plain-load or
- * bulk-copy variant; x-band, window and TMEM-staged variants give
+ * the same variant (per-CTA x windows included).  d_row (n+1), d_col and
+ * d_val (nnz) are device pointers, read during the call.  Options: val_kind
+ * F64 or F32, col_kind U32, kernel AUTO (the variant ispmv_plan_axt picks for
+ * the compacted AXT) or WIDE; x-band and TMEM-staged variants give
  * ISPMV_ERR_UNSUPPORTED.  The matrix is checked on the device before use:
  * a decreasing row pointer, row[0] != 0, row[n] != nnz or a column >= n
  * gives ISPMV_ERR_ARG.  Synchronises `stream`. */
@@ -349,15 +349,17 @@ int ispmv_plan_dev_csr(UIN n, UIN nnz, const UIN *d_row, const UIN *d_col, const
  * lengths, then copies into caller buffers (host or device; NULL skips an
  * array), synchronising `stream`.  val: slots_pad values of val_bytes each
  * (lane-interleaved when spl > 0), col: slots_pad, heads: slots_pad / 32
- * row-start words, segh: nseg, rowmap: nrowmap, empty: nempty.
+ * row-start words, segh: nseg, rowmap: nrowmap, empty: nempty; the per-CTA
+ * x windows of the window variants: nwin starts (lo) and lengths (len).
  * No reference counterpart. */
 typedef struct {
   uint64_t slots; uint64_t slots_pad; uint64_t seg_slots; uint64_t nseg;
-  uint64_t nrowmap; uint64_t nempty; UIN val_bytes; UIN spl;
+  uint64_t nrowmap; uint64_t nempty; UIN val_bytes; UIN spl; uint64_t nwin;
 } ispmv_plan_layout;
 int ispmv_plan_get_layout(ispmv_plan p, ispmv_plan_layout *l);
 int ispmv_plan_export_stream(ispmv_plan p, void *val, UIN *col, UIN *heads, UIN *segh, UIN *rowmap,
                              UIN *empty, void *stream);
+int ispmv_plan_export_windows(ispmv_plan p, UIN *lo, UIN *len, void *stream);
 
 /* y = A*x + beta*y with device pointers, beta in {0, 1}.  Stream-ordered.
  * A plan keeps per-product work areas on the device (segment records, the

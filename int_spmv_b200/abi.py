@@ -60,7 +60,8 @@ class PlanInfo(C.Structure):
 
 class PlanLayout(C.Structure):
     _fields_ = [("slots", C.c_uint64), ("slots_pad", C.c_uint64), ("seg_slots", C.c_uint64), ("nseg", C.c_uint64),
-                ("nrowmap", C.c_uint64), ("nempty", C.c_uint64), ("val_bytes", UIN), ("spl", UIN)]
+                ("nrowmap", C.c_uint64), ("nempty", C.c_uint64), ("val_bytes", UIN), ("spl", UIN),
+                ("nwin", C.c_uint64)]
 
 
 P_CSR = C.POINTER(StrMatCSR)
@@ -135,6 +136,7 @@ PROTOTYPES: dict[str, tuple] = {
     "ispmv_plan_dev_csr": (C.c_int, [UIN, UIN, VP, VP, VP, P_OPTS, P_PLAN, VP]),
     "ispmv_plan_get_layout": (C.c_int, [VP, C.POINTER(PlanLayout)]),
     "ispmv_plan_export_stream": (C.c_int, [VP, VP, VP, VP, VP, VP, VP, VP]),
+    "ispmv_plan_export_windows": (C.c_int, [VP, VP, VP, VP]),
     "ispmv_plan_destroy": (C.c_int, [VP]),
     "ispmv_plan_spmv": (C.c_int, [VP, VP, VP, C.c_int, VP]),
     "ispmv_plan_spmv_graph": (C.c_int, [VP, VP, VP, C.c_int, VP]),

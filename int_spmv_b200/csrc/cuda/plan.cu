@@ -24,6 +24,7 @@
 #include <vector>
 
 #include <cub/device/device_scan.cuh>
+#include <cub/device/device_segmented_radix_sort.cuh>
 
 #include "plan_tma.cuh"
 #include "spmm.cuh"
@@ -764,31 +765,125 @@ struct DevTmp {  // builder scratch, freed on every exit
   }
 };
 
-int dev_csr_stream(ispmv_plan_s *p, UIN n, UIN nnz, const UIN *row, const UIN *col, const FPT *val, cudaStream_t s) {
-  if (p->opts.kernel == ISPMV_KERNEL_AUTO) {
-    // the compacted AXT's default: 8 slots per lane for rows of fewer than
-    // 16 slots on average, else 16 (bulk-copy staged for FP64 values)
-    p->opts.kernel = ISPMV_KERNEL_WIDE;
-    if (p->opts.variant == 0) {
-      const bool long_rows = (double)nnz >= 16.0 * (double)n;
-      p->opts.variant = !long_rows ? 4 : p->opts.val_kind == ISPMV_VAL_F64 ? 11 : 0;
+// random_far_fraction on a device CSR: the same sample (nonzero
+// j = (size_t)(i * stride)), its row by binary search (the r with
+// row[r] <= j < row[r+1]), the same test; *far counts the hits.
+__global__ void dcsr_far(size_t S, double stride, UIN n, const UIN *__restrict__ row, const UIN *__restrict__ col,
+                         unsigned long long *__restrict__ far) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= S) return;
+  const size_t j = (size_t)(i * stride);
+  UIN a = 1, b = n;  // first k in [1, n] with row[k] > j (row[n] = nnz > j)
+  while (a < b) {
+    const UIN m = a + (b - a) / 2;
+    if (row[m] > j) b = m;
+    else a = m + 1;
+  }
+  const size_t r = a - 1;
+  const long long c = col[j];
+  if (llabs(c - (long long)r) <= 1536) return;
+  bool near_next = false;
+  if (r + 1 < n)
+    for (UIN k = row[r + 1]; k < row[r + 2] && !near_next; k++) near_next = llabs((long long)col[k] - c - 1) <= 16;
+  if (!near_next) atomicAdd(far, 1ull);
+}
+
+// Window keys: the column of every nonzero value, ~0 for a zero value
+// (sorted last, left out of the window choice as on the host).
+__global__ void dcsr_win_keys(size_t nnz, const UIN *__restrict__ col, const FPT *__restrict__ val,
+                              UIN *__restrict__ keys) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < nnz; q += stride)
+    keys[q] = val[q] != 0.0 ? col[q] : 0xFFFFFFFFu;
+}
+
+__global__ void dcsr_win_offsets(size_t nt, size_t T, size_t nnz, int *__restrict__ off) {
+  const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t <= nt) off[t] = (int)std::min(t * T, nnz);
+}
+
+// One CTA per plan CTA tile: stage_windows' choice from the tile's sorted
+// keys - the first i with the most keys in [cs[i], cs[i] + W - 1), the
+// interval centred on them, clamped to [0, ne - W], started at an even column.
+__global__ void __launch_bounds__(256) dcsr_windows(size_t nt, const int *__restrict__ off,
+                                                    const UIN *__restrict__ keys, UIN W, UIN ne,
+                                                    UIN *__restrict__ tlo, UIN *__restrict__ tlen) {
+  __shared__ UIN sb[8], si[8], sj[8];
+  const size_t t = blockIdx.x;
+  if (t >= nt) return;
+  if (ne <= W) {
+    if (threadIdx.x == 0) {
+      tlo[t] = 0;
+      tlen[t] = ne;
+    }
+    return;
+  }
+  const UIN *cs = keys + off[t];
+  const UIN all = (UIN)(off[t + 1] - off[t]);
+  UIN a = 0, b = all;  // m: keys below the sentinel
+  while (a < b) {
+    const UIN mid = a + (b - a) / 2;
+    if (cs[mid] == 0xFFFFFFFFu) b = mid;
+    else a = mid + 1;
+  }
+  const UIN m = a;
+  UIN best = 0, bi = 0xFFFFFFFFu, bj = 0;
+  for (UIN i = threadIdx.x; i < m; i += blockDim.x) {
+    const uint64_t lim = (uint64_t)cs[i] + (W - 1);
+    UIN lo = i, hi = m;  // first j in [i, m) with cs[j] >= lim
+    while (lo < hi) {
+      const UIN mid = lo + (hi - lo) / 2;
+      if ((uint64_t)cs[mid] < lim) lo = mid + 1;
+      else hi = mid;
+    }
+    if (lo - i > best) {
+      best = lo - i;
+      bi = i;
+      bj = lo;
     }
   }
-  const WideCfg wc = wide_variant(p->opts.variant);
-  if (p->opts.kernel != ISPMV_KERNEL_WIDE || p->opts.val_kind == ISPMV_VAL_F32_LO16 ||
-      p->opts.col_kind != ISPMV_COL_U32 || wc.win || wc.tmem || wc.stg)
-    return fail(ISPMV_ERR_UNSUPPORTED,
-                "plan from a device CSR: the lane-interleaved kernel (no x bands, windows or TMEM staging), "
-                "FP64/FP32 values, u32 columns");
-  p->fmt = F_CSR;
-  p->path = P_STREAM;
-  p->n = n;
-  p->nnz = nnz;
-  p->slots = nnz;
-  p->slots_pad = std::max(SS, (p->slots + SS - 1) / SS * SS);
-  p->seg_slots = p->opts.units_per_warp <= 0 ? wc.seg : seg_slots_of(p, 1);
-  if (p->seg_slots % SS) p->seg_slots = (p->seg_slots + SS - 1) / SS * SS;
-  p->nseg = (p->slots_pad + p->seg_slots - 1) / p->seg_slots;
+  // the largest count, the smallest i among equal counts
+  for (int d = 16; d > 0; d >>= 1) {
+    const UIN ob = __shfl_down_sync(FULL, best, d), oi = __shfl_down_sync(FULL, bi, d),
+              oj = __shfl_down_sync(FULL, bj, d);
+    if (ob > best || (ob == best && oi < bi)) {
+      best = ob;
+      bi = oi;
+      bj = oj;
+    }
+  }
+  const unsigned w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31u) == 0) {
+    sb[w] = best;
+    si[w] = bi;
+    sj[w] = bj;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (unsigned k = 1; k < blockDim.x / 32; k++)
+      if (sb[k] > best || (sb[k] == best && si[k] < bi)) {
+        best = sb[k];
+        bi = si[k];
+        bj = sj[k];
+      }
+    long long l = 0;
+    if (m > 0) {
+      const long long span = (long long)cs[bj - 1] - (long long)cs[bi] + 1;
+      l = (long long)cs[bi] - ((long long)W - span) / 2;
+    }
+    l = l < 0 ? 0 : l;
+    l = l > (long long)(ne - W) ? (long long)(ne - W) : l;
+    tlo[t] = (UIN)l & ~1u;
+    tlen[t] = W;
+  }
+}
+
+int dev_csr_stream(ispmv_plan_s *p, UIN n, UIN nnz, const UIN *row, const UIN *col, const FPT *val, cudaStream_t s) {
+  if (p->opts.kernel != ISPMV_KERNEL_AUTO && p->opts.kernel != ISPMV_KERNEL_WIDE)
+    return fail(ISPMV_ERR_UNSUPPORTED, "plan from a device CSR: the lane-interleaved kernel");
+  if (p->opts.val_kind == ISPMV_VAL_F32_LO16 || p->opts.col_kind != ISPMV_COL_U32)
+    return fail(ISPMV_ERR_UNSUPPORTED, "plan from a device CSR: FP64/FP32 values, u32 columns");
+  // the matrix is checked before any pass indexes through it
   DevTmp tmp;
   int *bad;
   UIN *flag, *pos;
@@ -812,6 +907,44 @@ int dev_csr_stream(ispmv_plan_s *p, UIN n, UIN nnz, const UIN *row, const UIN *c
   ISPMV_TRY(cudaMemcpyAsync(&nonempty, pos + n, sizeof nonempty, cudaMemcpyDeviceToHost, s));
   ISPMV_TRY(cudaStreamSynchronize(s));
   if (hbad) return fail(ISPMV_ERR_ARG, "plan from a device CSR: malformed row pointer or a column >= n");
+  if (p->opts.kernel == ISPMV_KERNEL_AUTO) {
+    // the compacted AXT's default (ispmv_plan_axt), with the scatter test
+    // run on the device sample
+    p->opts.kernel = ISPMV_KERNEL_WIDE;
+    if (p->opts.variant == 0) {
+      const bool long_rows = (double)nnz >= 16.0 * (double)n;
+      const bool plain = p->opts.val_kind == ISPMV_VAL_F64;
+      bool scattered = false;
+      const size_t S = std::min<size_t>(nnz, 1u << 16);
+      if (S) {
+        unsigned long long *dfar, hfar = 0;
+        TRY(tmp.alloc(1, &dfar));
+        ISPMV_TRY(cudaMemsetAsync(dfar, 0, sizeof *dfar, s));
+        dcsr_far<<<(unsigned)((S + 255) / 256), 256, 0, s>>>(S, (double)nnz / (double)S, n, row, col, dfar);
+        TRY(check_launch("dcsr_far"));
+        ISPMV_TRY(cudaMemcpyAsync(&hfar, dfar, sizeof hfar, cudaMemcpyDeviceToHost, s));
+        ISPMV_TRY(cudaStreamSynchronize(s));
+        scattered = (double)hfar / (double)S >= 0.05;
+      }
+      const int short_scattered = p->opts.val_kind == ISPMV_VAL_F32 ? 32 : 26;
+      p->opts.variant = !long_rows ? (scattered ? short_scattered : 4) : plain && !scattered ? 11 : 0;
+    }
+  }
+  const WideCfg wc = wide_variant(p->opts.variant);
+  if (wc.win || wc.tmem)
+    return fail(ISPMV_ERR_UNSUPPORTED,
+                "plan from a device CSR: the lane-interleaved kernel without x bands or TMEM staging");
+  if (wc.stg && nnz > 0x7FFFFFFFu)
+    return fail(ISPMV_ERR_UNSUPPORTED, "plan from a device CSR: per-CTA x windows up to 2^31 - 1 nonzeros");
+  p->fmt = F_CSR;
+  p->path = P_STREAM;
+  p->n = n;
+  p->nnz = nnz;
+  p->slots = nnz;
+  p->slots_pad = std::max(SS, (p->slots + SS - 1) / SS * SS);
+  p->seg_slots = p->opts.units_per_warp <= 0 ? wc.seg : seg_slots_of(p, 1);
+  if (p->seg_slots % SS) p->seg_slots = (p->seg_slots + SS - 1) / SS * SS;
+  p->nseg = (p->slots_pad + p->seg_slots - 1) / p->seg_slots;
   const unsigned spl = (unsigned)wc.spl;
   void *vi;
   if (p->opts.val_kind == ISPMV_VAL_F64) TRY(dev_alloc(p, p->slots_pad, reinterpret_cast<double **>(&vi)));
@@ -837,9 +970,44 @@ int dev_csr_stream(ispmv_plan_s *p, UIN n, UIN nnz, const UIN *row, const UIN *c
   TRY(check_launch("dcsr_rows"));
   dcsr_segh<<<(unsigned)((p->nseg + 255) / 256), 256, 0, s>>>(p->nseg, p->seg_slots, n, row, pos, p->segh);
   TRY(check_launch("dcsr_segh"));
+  size_t nt = 0;
+  if (wc.stg) {
+    // per-CTA x windows, as stage_windows picks them on the host
+    const UIN W = wc.cap & ~1u, ne = n & ~1u;
+    const size_t T = (size_t)WIDE_WARPS * p->seg_slots;
+    nt = std::max<size_t>(1, (p->nseg + WIDE_WARPS - 1) / WIDE_WARPS);
+    UIN *tlo, *tlen, *keys = nullptr, *sorted = nullptr;
+    int *off;
+    TRY(dev_alloc(p, nt, &tlo));
+    TRY(dev_alloc(p, nt, &tlen));
+    TRY(tmp.alloc(nt + 1, &off));
+    dcsr_win_offsets<<<(unsigned)((nt + 1 + 255) / 256), 256, 0, s>>>(nt, T, nnz, off);
+    TRY(check_launch("dcsr_win_offsets"));
+    if (ne > W && nnz) {
+      TRY(tmp.alloc(nnz, &keys));
+      TRY(tmp.alloc(nnz, &sorted));
+      dcsr_win_keys<<<gi, 256, 0, s>>>(nnz, col, val, keys);
+      TRY(check_launch("dcsr_win_keys"));
+      size_t sb = 0;
+      ISPMV_TRY(cub::DeviceSegmentedRadixSort::SortKeys(nullptr, sb, keys, sorted, (int)nnz, (int)nt, off, off + 1,
+                                                         0, 32, s));
+      void *sst;
+      TRY(tmp.alloc(sb, reinterpret_cast<unsigned char **>(&sst)));
+      ISPMV_TRY(cub::DeviceSegmentedRadixSort::SortKeys(sst, sb, keys, sorted, (int)nnz, (int)nt, off, off + 1, 0, 32,
+                                                         s));
+    }
+    dcsr_windows<<<(unsigned)nt, 256, 0, s>>>(nt, off, sorted, W, ne, tlo, tlen);
+    TRY(check_launch("dcsr_windows"));
+    p->xw.tlo = tlo;
+    p->xw.tlen = tlen;
+    p->xw.cap = W;
+    p->xw.nwin = 1;
+    p->xw.n = p->n;
+  }
   TRY(alloc_records(p));
+  if (wc.stg) p->xw.status = p->status;
   ISPMV_TRY(cudaStreamSynchronize(s));
-  p->info.device_bytes = (uint64_t)p->slots_pad * (vbytes(p) + 4) + p->slots_pad / 8;
+  p->info.device_bytes = (uint64_t)(8 * nt) + (uint64_t)p->slots_pad * (vbytes(p) + 4) + p->slots_pad / 8;
   return ISPMV_OK;
 }
 
@@ -870,6 +1038,19 @@ ISPMV_API int ispmv_plan_get_layout(ispmv_plan p, ispmv_plan_layout *l) {
   l->nempty = p->nempty;
   l->val_bytes = (UIN)vbytes(p);
   l->spl = p->opts.kernel == ISPMV_KERNEL_WIDE ? (UIN)wide_variant(p->opts.variant).spl : 0u;
+  l->nwin = p->opts.kernel == ISPMV_KERNEL_WIDE && wide_variant(p->opts.variant).stg
+                ? std::max<size_t>(1, (p->nseg + WIDE_WARPS - 1) / WIDE_WARPS)
+                : 0;
+  return ISPMV_OK;
+}
+
+ISPMV_API int ispmv_plan_export_windows(ispmv_plan p, UIN *lo, UIN *len, void *stream) {
+  ispmv_plan_layout l;
+  TRY(ispmv_plan_get_layout(p, &l));
+  cudaStream_t s = as_stream(stream);
+  if (l.nwin && lo) ISPMV_TRY(cudaMemcpyAsync(lo, p->xw.tlo, l.nwin * sizeof(UIN), cudaMemcpyDefault, s));
+  if (l.nwin && len) ISPMV_TRY(cudaMemcpyAsync(len, p->xw.tlen, l.nwin * sizeof(UIN), cudaMemcpyDefault, s));
+  ISPMV_TRY(cudaStreamSynchronize(s));
   return ISPMV_OK;
 }
 

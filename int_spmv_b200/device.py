@@ -162,6 +162,10 @@ class Plan:
         p = {k: (v.ctypes.data if v.size else None) for k, v in a.items()}
         check(lib.ispmv_plan_export_stream(self._h, p["val"], p["col"], p["heads"], p["segh"], p["rowmap"],
                                            p["empty"], _stream(stream)), "ispmv_plan_export_stream")
+        a["win_lo"], a["win_len"] = np.zeros(lay.nwin, np.uint32), np.zeros(lay.nwin, np.uint32)
+        if lay.nwin:
+            check(lib.ispmv_plan_export_windows(self._h, a["win_lo"].ctypes.data, a["win_len"].ctypes.data,
+                                                _stream(stream)), "ispmv_plan_export_windows")
         a["layout"] = {f: getattr(lay, f) for f, _ in abi.PlanLayout._fields_}
         return a
 

@@ -14,8 +14,9 @@ from paritylib import TOL_F32, TOL_F64, assert_parity
 
 pytestmark = pytest.mark.gpu
 
-# plain-load (4: 8 slots/lane; 0, 9: 16 slots/lane) and bulk-copy staged (11) variants
-VARIANTS = [4, 0, 9, 11]
+# plain-load (4: 8 slots/lane; 0, 9: 16 slots/lane), bulk-copy staged (11), per-CTA x
+# window (26), window + column prefetch (31) and column prefetch (32) variants
+VARIANTS = [4, 0, 9, 11, 26, 31, 32]
 
 
 def _dev(a):
@@ -41,7 +42,7 @@ def check_dev_plan(row, col, val, x, val_kind, variant, units_per_warp=0, kernel
     if ph is not None:
         b = ph.export_stream()
         assert a["layout"] == b["layout"]
-        for k in ("val", "col", "heads", "segh", "rowmap", "empty"):
+        for k in ("val", "col", "heads", "segh", "rowmap", "empty", "win_lo", "win_len"):
             assert np.array_equal(a[k], b[k]), k
         assert chosen["device_bytes"] == ph.info["device_bytes"]
         assert chosen["alg_bytes"] == ph.info["alg_bytes"]
@@ -77,16 +78,35 @@ def test_dev_plan_random_and_segments(variant):
             check_dev_plan(row, col, val, x, "f64", variant, units_per_warp=upw)
 
 
-def test_dev_plan_auto_picks_the_compacted_default():
-    """kernel=auto: 8 slots per lane for short rows, the bulk-copy staged
-    16-slot form for FP64 rows of 16 slots or more (as ispmv_plan_axt)."""
+@pytest.mark.parametrize("val_kind", ["f64", "f32"])
+def test_dev_plan_auto_picks_the_compacted_default(val_kind):
+    """kernel=auto picks the kernel ispmv_plan_axt picks for the compacted
+    AXT of the same matrix, the scatter test run on the device: short
+    scattered rows (per-CTA window / column prefetch), short rows on fixed
+    far diagonals, long structured rows (bulk-copy staged for FP64) and long
+    scattered rows."""
+    import torch
+
+    from int_spmv_b200 import device as D
+    from int_spmv_b200 import formats as F
     from int_spmv_b200 import matrices as M
-    row, col, val = M.random_csr(5001, 3, rl_max=20, empty_frac=0.05)
-    p = check_dev_plan(row, col, val, M.uniform_x(5001, 3), "f64", 0, kernel="auto")
-    assert p.export_stream()["layout"]["spl"] == 8
-    row, col, val = M.stencil27(20, seed=2)
-    p = check_dev_plan(row, col, val, M.uniform_x(8000, 3), "f64", 0, kernel="auto")
-    assert p.export_stream()["layout"]["spl"] == 16
+    n = 20000
+    r = np.repeat(np.arange(n), 3)
+    c = (r + np.tile([-1700, 0, 1700], n)) % n
+    order = np.lexsort((c, r))
+    diag = (np.arange(0, 3 * n + 1, 3, dtype=np.uint32), c[order].astype(np.uint32),
+            np.random.default_rng(2).normal(size=3 * n))
+    mats = [M.random_csr(5001, 3, rl_max=20, empty_frac=0.05), diag, M.stencil27(20, seed=2),
+            M.random_csr(6001, 5, rl_max=60, empty_frac=0.05)]
+    for row, col, val in mats:
+        x = M.uniform_x(len(row) - 1, 3)
+        pd = check_dev_plan(row, col, val, x, val_kind, 0, kernel="auto")
+        csr = F.CSR(row, col, val)
+        ph = D.Plan(csr, F.getFormatDataAXT(0, 128, 8, 1, "COM", csr, x)[1], val=val_kind)
+        xt = torch.from_numpy(x).cuda()
+        pd.spmv(xt)
+        ph.spmv(xt)
+        assert pd.kernel_name() == ph.kernel_name(), (pd.kernel_name(), ph.kernel_name())
 
 
 def test_dev_plan_rejects_malformed_and_unsupported():
