@@ -109,3 +109,27 @@ def test_sta_report_matches_reference(tmp_path, name):
         if a.startswith("name:"):
             continue  # the file name itself differs
         assert a == b
+
+
+def test_plan_layout_struct_matches_header():
+    """ispmv_plan_layout's C layout (six u64 lengths, val_bytes, spl, then
+    the window count) as the ctypes mirror declares it: 64 bytes, nwin last
+    at offset 56."""
+    assert C.sizeof(abi.PlanLayout) == 64
+    assert abi.PlanLayout.nwin.offset == 56
+
+
+def test_plan_from_device_csr_checks_shapes_before_any_device_call():
+    """Plan.from_device_csr rejects inconsistent array lengths and a
+    non-FP64 value array on the host, before the library is called."""
+    import torch
+
+    from int_spmv_b200 import device as D
+    row = torch.tensor([0, 1, 2], dtype=torch.int32)
+    col = torch.tensor([0, 1], dtype=torch.int32)
+    with pytest.raises(ValueError):
+        D.Plan.from_device_csr(row, col, torch.zeros(3, dtype=torch.float64))
+    with pytest.raises(ValueError):
+        D.Plan.from_device_csr(row, col, torch.zeros(2, dtype=torch.float32))
+    with pytest.raises(ValueError):
+        D.Plan.from_device_csr(torch.tensor([0], dtype=torch.int32), col[:0], torch.zeros(0, dtype=torch.float64))
