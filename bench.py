@@ -461,7 +461,8 @@ def main(argv=None):
                                       "f32": "FP32 values, FP32 multiply, FP64 accumulate",
                                       "f32lo": "FP32 values + BF16 lo-word, FP64 accumulate"}[a.val] +
                                      (", u32 columns" if a.col == "u32" else ", 16-bit column deltas"),
-                       "kernel_variant": plan.info["kernel"],
+                       "kernel_family": {0: "auto", 1: "ldg", 2: "tma", 3: "rows", 4: "wide"}.get(plan.info["kernel"], "?"),
+                       "kernel": kname,
                        "l2": "no flush: inputs larger than L2 (%.0f MB algorithmic bytes per step)" % (B / 1e6),
                        "parallelism": f"replicas x{ws} (one full matrix per GPU, no collective)"},
             "gb_per_s": gbs,
