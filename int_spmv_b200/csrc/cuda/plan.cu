@@ -349,7 +349,8 @@ double random_far_fraction(const str_matCSR *csr) {
   size_t far = 0;
   for (size_t i = 0, r = 0; i < S; i++) {
     const size_t j = (size_t)(i * stride);
-    while (csr->row[r + 1] <= j) r++;
+    while (r < csr->nrows && csr->row[r + 1] <= j) r++;
+    if (r >= csr->nrows) break;  // a row pointer that does not cover nnz
     const long long c = csr->col[j];
     if (std::llabs(c - (long long)r) <= 1536) continue;
     bool near_next = false;
