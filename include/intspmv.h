@@ -217,9 +217,12 @@ int ispmv_dev_int_axt_com_h1(UIN bn, UIN bs, UIN log, UIN thw, UIN tn, UIN lenAX
  * ISPMV_K1_NOALLOC_MAX_ROWS doubles (8 MiB), held by every GPU that loads
  * the library until the process exits.  Arrays are those of str_matK1 on
  * the device; vec and y have nrows entries; chunkNum = ceil(nrows / 8).
- * More rows than the maximum is rejected with ISPMV_ERR_ARG.  The first call
- * on each device looks up the array's device address (cudaGetSymbolAddress),
- * so make that first call before any stream capture.  Calls share the
+ * More rows than the maximum, or a null array, is rejected with
+ * ISPMV_ERR_ARG before anything is launched.  The first call in a device's
+ * context looks up the array's device address (cudaGetSymbolAddress); the
+ * address is kept for that context and looked up again in a new one (after
+ * cudaDeviceReset, say), so make the first call on each device, and the
+ * first after a reset, before any stream capture.  Calls share the
  * array: calls that overlap on the GPU (concurrent streams, or several host
  * threads) race and must be serialised by the caller.  Nothing needs
  * clearing between calls: every call writes the part of the array it reads. */

@@ -23,6 +23,8 @@
 //                   segment, so row-0 segments whose descriptor is 0 are
 //                   summed (the reference skips them, M:1555) and segment
 //                   sums are true sums, not prefix differences (M:1559).
+#include <cuda.h>
+
 #include <cstdio>
 #include <cstdlib>
 #include <mutex>
@@ -229,7 +231,7 @@ ISPMV_API int ispmv_dev_int_axc(UIN nrows, const FPT *ax, const UIN *brp, FPT *y
 ISPMV_API int ispmv_dev_int_k1(UIN chunkNum, const FPT *val, const UIN *col, const UIN *chp, const UIN *nmc,
                                const FPT *vec, FPT *res, void *stream) {
   if (chunkNum == 0) return ISPMV_OK;
-  if (!chp || !nmc || !vec || !res) return ISPMV_ERR_ARG;
+  if (!val || !col || !chp || !nmc || !vec || !res) return ISPMV_ERR_ARG;
   lit::k_k1<false><<<lit::blocks_for((size_t)chunkNum * 8), lit::TPB, 0, as_stream(stream)>>>(
       chunkNum, 0xFF, val, col, chp, nmc, nullptr, vec, res);
   return check_launch("ispmv_dev_int_k1");
@@ -245,7 +247,7 @@ ISPMV_API int ispmv_dev_order_k1(UIN len, const UIN *permi, const FPT *arrDis, F
 ISPMV_API int ispmv_dev_int_k1p(unsigned char mask, UIN chunkNum, const FPT *val, const UIN *col, const UIN *chp,
                                 const UIN *nmc, const UIN *permi, const FPT *vec, FPT *res, void *stream) {
   if (chunkNum == 0) return ISPMV_OK;
-  if (!chp || !nmc || !permi || !vec || !res) return ISPMV_ERR_ARG;
+  if (!val || !col || !chp || !nmc || !permi || !vec || !res) return ISPMV_ERR_ARG;
   lit::k_k1<true><<<lit::blocks_for((size_t)chunkNum * 8), lit::TPB, 0, as_stream(stream)>>>(
       chunkNum, mask, val, col, chp, nmc, permi, vec, res);
   return check_launch("ispmv_dev_int_k1p");
@@ -289,23 +291,69 @@ ISPMV_API int ispmv_dev_int_axt_com_h1(UIN bn, UIN bs, UIN log, UIN thw, UIN tn,
 static __device__ __align__(256) double g_k1_rows[ISPMV_K1_NOALLOC_MAX_ROWS];
 
 namespace {
+// The array's device address, per device, with the id of the context it was
+// looked up in.  A context that is destroyed and created again (for one,
+// after cudaDeviceReset) loads the module afresh, possibly at another
+// address, and gets a new id: the address is then looked up again.
+struct K1RowsAddr {
+  unsigned long long ctx_id;
+  double *addr;
+};
 std::mutex g_k1_rows_mu;
-double *g_k1_rows_addr[64] = {nullptr};  // the array's device address, per device
+K1RowsAddr g_k1_rows_addr[64] = {};
 
-// The array's address on the current device, looked up once per device with
-// that device current (the host-side symbol is not a device address).
+// cuCtxGetCurrent / cuCtxGetId through the runtime's driver entry points, so
+// the library links no driver library.  Null when unavailable.
+typedef CUresult(CUDAAPI *CtxGetCurrentFn)(CUcontext *);
+typedef CUresult(CUDAAPI *CtxGetIdFn)(CUcontext, unsigned long long *);
+CtxGetCurrentFn g_ctx_current = nullptr;
+CtxGetIdFn g_ctx_id = nullptr;
+std::once_flag g_ctx_fns_once;
+
+void find_ctx_fns() {
+  void *f = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+      q == cudaDriverEntryPointSuccess)
+    g_ctx_current = reinterpret_cast<CtxGetCurrentFn>(f);
+  f = nullptr;
+  if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+      q == cudaDriverEntryPointSuccess)
+    g_ctx_id = reinterpret_cast<CtxGetIdFn>(f);
+  (void)cudaGetLastError();
+}
+
+// Id of the calling thread's current context; 0 when there is none yet or
+// the driver entry points are unavailable.
+unsigned long long current_ctx_id() {
+  std::call_once(g_ctx_fns_once, find_ctx_fns);
+  if (!g_ctx_current || !g_ctx_id) return 0;
+  CUcontext c = nullptr;
+  unsigned long long id = 0;
+  if (g_ctx_current(&c) != CUDA_SUCCESS || !c) return 0;
+  if (g_ctx_id(c, &id) != CUDA_SUCCESS) return 0;
+  return id;
+}
+
+// The array's address in the current context (the host-side symbol is not a
+// device address).  Looked up with cudaGetSymbolAddress the first time a
+// context of this device calls, then reused while that context lives; with
+// no context id available it is looked up on every call.
 int k1_rows_scratch(double **out) {
   int dev = 0;
   ISPMV_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return fail(ISPMV_ERR_UNSUPPORTED, "ispmv_dev_k1_spmv_noalloc: device index >= 64");
   std::lock_guard<std::mutex> g(g_k1_rows_mu);
-  if (!g_k1_rows_addr[dev]) {
+  K1RowsAddr &c = g_k1_rows_addr[dev];
+  const unsigned long long id = current_ctx_id();
+  if (!c.addr || id == 0 || id != c.ctx_id) {
     void *addr = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&addr, g_k1_rows);
     if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(g_k1_rows)");
-    g_k1_rows_addr[dev] = static_cast<double *>(addr);
+    c.addr = static_cast<double *>(addr);
+    c.ctx_id = current_ctx_id();  // the lookup makes the device's context current if none was
   }
-  *out = g_k1_rows_addr[dev];
+  *out = c.addr;
   return ISPMV_OK;
 }
 }  // namespace
@@ -313,7 +361,8 @@ int k1_rows_scratch(double **out) {
 ISPMV_API int ispmv_dev_k1_spmv_noalloc(UIN nrows, UIN chunkNum, const FPT *val, const UIN *col, const UIN *chp,
                                         const UIN *nmc, const UIN *permi, const FPT *vec, FPT *y, void *stream) {
   if (nrows == 0) return ISPMV_OK;
-  if (!chp || !nmc || !permi || !vec || !y) return ISPMV_ERR_ARG;
+  if (!val || !col || !chp || !nmc || !permi || !vec || !y)
+    return fail(ISPMV_ERR_ARG, "ispmv_dev_k1_spmv_noalloc: null array");
   if ((uint64_t)chunkNum * 8 < nrows || (uint64_t)chunkNum * 8 >= (uint64_t)nrows + 8)
     return fail(ISPMV_ERR_ARG, "ispmv_dev_k1_spmv_noalloc: chunkNum must be ceil(nrows / 8)");
   if ((uint64_t)chunkNum * 8 > ISPMV_K1_NOALLOC_MAX_ROWS)

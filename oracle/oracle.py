@@ -28,10 +28,27 @@ U32, F64 = np.uint32, np.float64
 P_U, P_D = C.POINTER(C.c_uint), C.POINTER(C.c_double)
 
 
+# Where this build environment keeps the reference checkout when
+# $INTSPMV_REF_DIR does not name one (read only by this build step).
+_REF_CHECKOUT = "/root/reference"
+
+
+def ref_dir() -> str | None:
+    """The reference checkout to compile oracle/_ref from: $INTSPMV_REF_DIR,
+    else the build environment's checkout when present, else None (a
+    prebuilt oracle/_ref is then kept, as on a machine without the source)."""
+    d = os.environ.get("INTSPMV_REF_DIR") or _REF_CHECKOUT
+    return d if os.path.exists(os.path.join(d, "intSpmv_main.c")) else None
+
+
 def build(quiet: bool = True) -> None:
     """make -C oracle: the restatement always, the reference when its source
     is present (otherwise a prebuilt _ref library is kept)."""
-    r = subprocess.run(["make", "-C", str(HERE)], capture_output=True, text=True)
+    cmd = ["make", "-C", str(HERE)]
+    rd = ref_dir()
+    if rd:
+        cmd.append(f"REF_DIR={rd}")
+    r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"oracle build failed:\n{r.stdout}\n{r.stderr}")
     if not quiet:

@@ -20,6 +20,15 @@ def _csr(g):
     return F.CSR(g["row"], g["col"], g["val"])
 
 
+def _same_fd(fd, name, expect):
+    """Formats-table row: the name, the memory footprint and the occupancy
+    (beta, NaN in both when the format holds no slot), exactly."""
+    mfp, beta = (float(v) for v in expect)
+    assert fd.name == name
+    assert fd.mfp == mfp
+    assert (np.isnan(fd.beta) and np.isnan(beta)) or fd.beta == beta, (fd.beta, beta)
+
+
 @pytest.mark.parametrize("name", golden_names())
 def test_stats(name):
     g = load_golden(name)
@@ -35,7 +44,7 @@ def test_axc(name):
     c = _csr(g)
     fd, m = F.getFormatDataAXC(0, c, g["x"])
     assert np.array_equal(m.brp, g["axc_brp"]) and np.array_equal(m.ax, g["axc_ax"])
-    assert fd.name == "AXC" and [fd.mfp, fd.beta] == list(g["axc_fd"]) or np.isnan(fd.beta)
+    _same_fd(fd, "AXC", g["axc_fd"])
     # column companion: every value slot's column, 0 on padding
     axi = m.cols()
     v = m.ax.reshape(-1, 16)[:, :8].reshape(-1)
@@ -51,7 +60,7 @@ def test_k1(name):
     fd, m = F.getFormatDataK1(8, c, g["x"])
     for f in ("permi", "nmc", "chp", "val", "col"):
         assert np.array_equal(getattr(m, f), g["k1_" + f]), f
-    assert fd.name == "K1" and fd.mfp == g["k1_fd"][0]
+    _same_fd(fd, "K1", g["k1_fd"])
     assert m.mask == int(g["k1_mask"])
 
 
@@ -69,8 +78,7 @@ def test_axt(name, mode, th, bs):
     assert (m.c.tileN, m.c.lenAX, m.c.lenSEC, m.c.lenCON, m.c.logTH) == (tileN, lenAX, lenSEC, lenCON, logTH)
     if mode == "COM":
         assert m.c.log == log
-    assert fd.name == str(g[key + "_name"])
-    assert fd.mfp == g[key + "_fd"][0]
+    _same_fd(fd, str(g[key + "_name"]), g[key + "_fd"])
     # companion columns agree with the x copies wherever x is distinct per column
     axi = m.cols()
     v = m.ax.reshape(-1, 16)[:, :8].reshape(-1)

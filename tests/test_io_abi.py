@@ -133,3 +133,19 @@ def test_plan_from_device_csr_checks_shapes_before_any_device_call():
         D.Plan.from_device_csr(row, col, torch.zeros(2, dtype=torch.float32))
     with pytest.raises(ValueError):
         D.Plan.from_device_csr(torch.tensor([0], dtype=torch.int32), col[:0], torch.zeros(0, dtype=torch.float64))
+
+
+def test_k1_entry_points_reject_null_arrays_before_any_device_call():
+    """The device K1 entry points check their arrays on the host: a null
+    value or column array is ISPMV_ERR_ARG, returned before anything is
+    launched (so this needs no GPU).  Any non-null address passes the check,
+    which is all these calls read before returning."""
+    lib = load()
+    p = C.c_void_p(16)  # never dereferenced: the null check fails first
+    nul = C.c_void_p(0)
+    assert lib.ispmv_dev_k1_spmv_noalloc(16, 2, nul, p, p, p, p, p, p, None) == 1
+    assert lib.ispmv_dev_k1_spmv_noalloc(16, 2, p, nul, p, p, p, p, p, None) == 1
+    assert lib.ispmv_dev_int_k1(2, nul, p, p, p, p, p, None) == 1
+    assert lib.ispmv_dev_int_k1(2, p, nul, p, p, p, p, None) == 1
+    assert lib.ispmv_dev_int_k1p(0xFF, 2, nul, p, p, p, p, p, p, None) == 1
+    assert lib.ispmv_dev_int_k1p(0xFF, 2, p, nul, p, p, p, p, p, None) == 1

@@ -80,6 +80,32 @@ def test_noalloc_matches_allocating_pair(env, case):
         assert_parity(a, orc.cf_csr(row, col, val, x), absax, what=f"noalloc vs oracle, call {call}")
 
 
+def test_noalloc_allocates_nothing(env):
+    """Repeated calls after the first leave the device's free memory as it
+    was: the scratch is the static array, nothing else is allocated."""
+    torch, D, F, orc, lib = env
+    from int_spmv_b200 import matrices as M
+    row, col, val = M.poisson2d(200)
+    n = len(row) - 1
+    x = M.uniform_x(n, 5)
+    nrows, cn, (kval, kcol, kchp, knmc, kperm) = _k1_arrays(D, F, row, col, val, x)
+    xt = torch.from_numpy(x).cuda()
+    y = torch.empty(n, dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    args = (nrows, cn, kval.data_ptr(), kcol.data_ptr(), kchp.data_ptr(), knmc.data_ptr(), kperm.data_ptr(),
+            xt.data_ptr(), y.data_ptr(), stream)
+    assert lib.ispmv_dev_k1_spmv_noalloc(*args) == 0  # the first call may load the library's kernels
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(5):
+        assert lib.ispmv_dev_k1_spmv_noalloc(*args) == 0
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+    assert_parity(y.cpu().numpy(), orc.cf_csr(row, col, val, x), orc.abs_csr(row, col, val, x),
+                  what="noalloc after repeated calls")
+
+
 def test_noalloc_rejects_beyond_maximum(env):
     torch, D, F, orc, lib = env
     from int_spmv_b200._lib import load
@@ -90,4 +116,8 @@ def test_noalloc_rejects_beyond_maximum(env):
     assert st == 1
     assert b"ISPMV_K1_NOALLOC_MAX_ROWS" in load().ispmv_last_error()
     st = lib.ispmv_dev_k1_spmv_noalloc(16, 3, p, p, p, p, p, p, p, None)  # chunkNum != ceil(16/8)
+    assert st == 1
+    st = lib.ispmv_dev_k1_spmv_noalloc(16, 2, None, p, p, p, p, p, p, None)  # null values
+    assert st == 1
+    st = lib.ispmv_dev_k1_spmv_noalloc(16, 2, p, None, p, p, p, p, p, None)  # null columns
     assert st == 1
