@@ -81,6 +81,28 @@ def build_format(F, csr, x, fmt: str):
     raise ValueError(fmt)
 
 
+VALUE_KIND = {"f64": "FP64 values, FP64 accumulate", "f32": "FP32 values, FP32 multiply, FP64 accumulate",
+              "f32lo": "FP32 values + BF16 lo-word, FP64 accumulate"}
+
+
+def run_config(wl, fmt_name: str, val: str, col: str, B: float) -> dict:
+    """The workload both arms run (ours and --impl reference print the same
+    dict): matrix, format, value and column form, L2 handling."""
+    return {"workload": wl["name"], "format": fmt_name, "n": len(wl["row"]) - 1, "nnz": len(wl["col"]),
+            "value_kind": VALUE_KIND[val] + (", u32 columns" if col == "u32" else ", 16-bit column deltas"),
+            "l2": "no flush: inputs larger than L2 (%.0f MB algorithmic bytes per step)" % (B / 1e6),
+            "parallelism": "replicas (one full matrix per process, no collective)"}
+
+
+def format_name(fmt: str) -> str:
+    """The reference's name of a bench format (getFormatData*, intSpmv_main.c:324-1381)."""
+    if fmt in ("CSR", "AXC", "K1", "K1P"):
+        return fmt
+    if fmt.startswith("NOC"):
+        return f"AXT_NOC_H{int(fmt[3:])}_HW8"
+    return f"AXT_COM_H1_HW8_BS{int(fmt[3:])}"
+
+
 def alg_bytes(n: int, nnz: int, bval: int = 8) -> float:
     """nnz*(b_val + b_idx) + n*(b_x + b_y) + 4*(n+1)."""
     return nnz * (bval + 4.0) + n * 16.0 + 4.0 * (n + 1)
@@ -258,6 +280,8 @@ def main(argv=None):
     ap.add_argument("--batch-nmax", type=float, default=2e5, help="largest n of the batched matrices")
     ap.add_argument("--no-formats", action="store_true", help="skip the per-format table")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-precision", action="store_true",
+                    help="skip the FP64 / FP32-value lines on the 27-point stencil 160^3")
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of reference CPU work")
     a = ap.parse_args(argv)
     rank, local_rank, ws = dist_env()
@@ -369,15 +393,27 @@ def main(argv=None):
             k = max(20, min(a.steps, 400))
             s_, _ = timed(lambda: p.spmv(x, y), k, 5, ws, stream, dev)
             t = s_ / k
+            # the main kernel alone (event pairs); for K1 the rest of the step
+            # is the reorder pass, the reference's ordTime (intSpmv_main.c:1001-1016)
+            p.time_kernels(k)
+            timed(lambda: p.spmv(x, y), k, 3, ws, stream, dev)
+            kms_, kn_ = p.kernel_ms()
+            p.time_kernels(0)
+            tk = kms_ / 1e3 / max(kn_, 1)
             bb = p.info["alg_bytes"]
             kid = {0: "auto", 1: "ldg", 2: "tma", 3: "rows", 4: "wide"}.get(p.info["kernel"], "?")
             row_ = {"ms": t * 1e3, "gflops": flops / t / 1e9, "gbs": bb / t / 1e9, "frac": bb / t / 1e9 / peak,
-                    "kernel": p.kernel_name()}
+                    "kernel_ms": tk * 1e3, "kernel_frac": bb / tk / 1e9 / peak, "kernel": p.kernel_name()}
+            if f == "K1":
+                row_["ord_ms"] = max(0.0, (t - tk) * 1e3)
             if check is not None:
                 p.spmv(x, y)
-                e_ = np.abs(y.cpu().numpy() - yr)
+                yh = y.cpu().numpy()
+                e_ = np.abs(yh - yr)
                 row_["max_componentwise_err"] = float(np.max(e_ / np.maximum(ab, 1e-300)))
                 row_["normwise_err"] = float(np.linalg.norm(e_) / np.linalg.norm(yr))
+                aerr, rerr, pos = F.getErrors(yr, yh)  # the reference's own columns (intSpmv_main.c:404-425)
+                row_.update(aErr=aerr, rErr=rerr, pos=int(pos))
             formats[f"{p.info['name']}/{vk}/{ck}/{kid}"] = row_
             del p
         # the vendor library on the same CSR, as a comparison row only (never
@@ -398,6 +434,16 @@ def main(argv=None):
             del A
         except Exception as e:  # the comparison row must not sink the run
             formats["cuSPARSE_CSR/f64/i32/library"] = {"unavailable": str(e)[:120]}
+
+    # the precision target on the 27-point stencil 160^3: plain FP64 against
+    # the reduced-byte forms, each with the kernel AUTO picks, its own
+    # algorithmic bytes and its error against the FP64 oracle
+    precision = None
+    if not a.no_precision and a.workload != "stencil160":
+        try:
+            precision = precision_lines(a, rank, ws, stream, dev, peak)
+        except Exception as e:  # the extra lines must not sink the headline
+            precision = {"unavailable": str(e)[:160]}
 
     # format conversion: the host builder (OpenMP, the reference's layout
     # rules) against the same conversion on the GPU, for the compacted AXT
@@ -456,15 +502,9 @@ def main(argv=None):
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": {"f64": "f64", "f32": "f32-mul/f64-acc", "f32lo": "f32+bf16lo-mul/f64-acc"}[a.val],
             "data": f"synthetic: {wl['desc']} (int_spmv_b200/matrices.py)",
-            "config": {"workload": wl["name"], "format": fmt_name, "n": n, "nnz": nnz,
-                       "value_kind": {"f64": "FP64 values, FP64 accumulate",
-                                      "f32": "FP32 values, FP32 multiply, FP64 accumulate",
-                                      "f32lo": "FP32 values + BF16 lo-word, FP64 accumulate"}[a.val] +
-                                     (", u32 columns" if a.col == "u32" else ", 16-bit column deltas"),
-                       "kernel_family": {0: "auto", 1: "ldg", 2: "tma", 3: "rows", 4: "wide"}.get(plan.info["kernel"], "?"),
-                       "kernel": kname,
-                       "l2": "no flush: inputs larger than L2 (%.0f MB algorithmic bytes per step)" % (B / 1e6),
-                       "parallelism": f"replicas x{ws} (one full matrix per GPU, no collective)"},
+            "config": run_config(wl, fmt_name, a.val, a.col, alg_bytes(n, nnz, {"f64": 8, "f32": 4, "f32lo": 4}[a.val])),
+            "kernel": {"family": {0: "auto", 1: "ldg", 2: "tma", 3: "rows", 4: "wide"}.get(plan.info["kernel"], "?"),
+                       "name": kname, "replicas": ws},
             "gb_per_s": gbs,
             "roofline": {"bound": "hbm", "achieved": kern_gbs, "peak": peak, "unit": "GB/s",
                          "frac": kern_gbs / peak, "traffic": traffic_for(f"{wl['name']}/{a.format}/{kname}"),
@@ -479,6 +519,7 @@ def main(argv=None):
             "clocks": clocks,
             "parity": check,
             "formats": formats,
+            "precision": precision,
             "conversion": conversion,
         }
         print(json.dumps(out), flush=True)
@@ -486,6 +527,61 @@ def main(argv=None):
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
+
+
+def precision_lines(a, rank, ws, stream, dev, peak):
+    """FP64 against the reduced-byte forms on the 3D 27-point stencil 160^3
+    (n = 4,096,000, nnz = 109,215,352; diagonal 26, off-diagonal
+    -1 + U[-0.1, 0.1], seed 2), compacted AXT bs 128, each form on the kernel
+    AUTO picks: step and main-kernel time, GB/s of the form's own
+    algorithmic bytes (b_val = 8 or 4, b_idx = 4, or 2 + the per-batch bases
+    for 16-bit deltas), the fraction of the HBM peak, and the error against
+    the FP64 oracle; then the speed-up of each form over FP64."""
+    import torch
+
+    from int_spmv_b200 import device as D
+    from int_spmv_b200 import formats as F
+    wl = make_workload("stencil160")
+    csr = F.CSR(wl["row"], wl["col"], wl["val"])
+    com = F.getFormatDataAXT(0, 128, 8, 1, "COM", csr, wl["x"])[1]
+    x = torch.from_numpy(wl["x"]).to(dev)
+    y = torch.empty(csr.n, dtype=torch.float64, device=dev)
+    yr = ab = None
+    if rank == 0:
+        from oracle import Oracle
+        orc = Oracle()
+        yr = orc.cf_csr(wl["row"], wl["col"], wl["val"], wl["x"])
+        ab = orc.abs_csr(wl["row"], wl["col"], wl["val"], wl["x"])
+    k = max(200, min(a.steps, 2000))
+    out = {"workload": wl["name"], "n": csr.n, "nnz": csr.nnz, "format": "AXT_COM_H1_HW8_BS128", "steps": k}
+    for vk, ck in (("f64", "u32"), ("f32", "u32"), ("f32", "d16"), ("f64", "d16"), ("f32lo", "u32")):
+        p = D.Plan(csr, com, val=vk, col=ck)
+        s_, _ = timed(lambda: p.spmv(x, y), k, 5, ws, stream, dev)
+        p.time_kernels(k)
+        timed(lambda: p.spmv(x, y), k, 3, ws, stream, dev)
+        kms, kn = p.kernel_ms()
+        p.time_kernels(0)
+        t, tk = s_ / k, kms / 1e3 / max(kn, 1)
+        bb = p.info["alg_bytes"]
+        row = {"ms": t * 1e3, "kernel_ms": tk * 1e3, "gflops": 2.0 * csr.nnz / t / 1e9, "alg_bytes": bb,
+               "gbs": bb / tk / 1e9, "frac": bb / tk / 1e9 / peak, "kernel": p.kernel_name(),
+               "bound": 1e-12 if vk == "f64" else 1e-6}
+        if rank == 0:
+            p.spmv(x, y)
+            yh = y.cpu().numpy()
+            e = np.abs(yh - yr)
+            row["max_componentwise_err"] = float(np.max(e / np.maximum(ab, 1e-300)))
+            row["normwise_err"] = float(np.linalg.norm(e) / np.linalg.norm(yr))
+            row["pass"] = bool(np.all(e <= row["bound"] * ab))
+            aerr, rerr, pos = F.getErrors(yr, yh)
+            row.update(aErr=aerr, rErr=rerr, pos=int(pos))
+        out[f"{vk}/{ck}"] = row
+        del p
+    base = out["f64/u32"]
+    out["speedup_vs_f64"] = {f: {"step": base["ms"] / out[f]["ms"], "kernel": base["kernel_ms"] / out[f]["kernel_ms"]}
+                             for f in ("f32/u32", "f32/d16", "f64/d16", "f32lo/u32")}
+    out["target"] = "FP32 values / FP64 accumulate >= 1.4x plain FP64 at <= 1e-6 relative error"
+    return out
 
 
 def _event_time(fn, steps: int, warmup: int) -> float:
@@ -516,6 +612,7 @@ def main_spmm(a, rank, ws, W):
     csr = F.CSR(wl["row"], wl["col"], wl["val"])
     n, nnz = csr.n, csr.nnz
     orc = Oracle()
+    peak, peak_src = hbm_peak()
     res, launches = {}, 0
     for val in ("f64", "f32"):
         for k in (8, 16, 32):
@@ -534,8 +631,10 @@ def main_spmm(a, rank, ws, W):
                 ref, ab = orc.cf_csr(wl["row"], wl["col"], wl["val"], xj), orc.abs_csr(wl["row"], wl["col"], wl["val"], xj)
                 err = max(err, float(np.max(np.abs(Yh[:, j] - ref) / np.maximum(ab, 1e-300))))
             bval = 8 if val == "f64" else 4
+            # nnz*(b_val + b_idx) + n*k*(b_x + b_y) + 4*(n+1): A read once, X and Y once
             B = nnz * (bval + 4) + n * k * 16 + 4 * (n + 1)
             res[f"{val}/k{k}"] = {"ms": t * 1e3, "gflops": 2 * nnz * k / t / 1e9, "gbs": B / t / 1e9,
+                                  "alg_bytes": B, "frac": B / t / 1e9 / peak, "kernel": plan.kernel_name(),
                                   "format": choice["format"], "kwargs": choice["kwargs"],
                                   "max_componentwise_err": err, "rhs_columns_checked": 3}
             del plan
@@ -545,7 +644,11 @@ def main_spmm(a, rank, ws, W):
            "vs_baseline": None, "dtype": "f64", "data": "synthetic: power-law n=1,000,000 seed 3, X~U[-1,1]",
            "config": {"workload": "spmm_powerlaw_n1M_seed3", "n": n, "nnz": nnz, "k": [8, 16, 32],
                       "choice": "autotuned per (value form, k)"},
-           "gpu_launches": launches, "results": res}
+           "gpu_launches": launches,
+           "roofline": {"bound": "hbm", "achieved": best["gbs"], "peak": peak, "unit": "GB/s",
+                        "frac": best["frac"], "traffic": None, "kernel": best["kernel"], "peak_source": peak_src,
+                        "note": "achieved = (nnz*(b_val+4) + n*k*16 + 4*(n+1)) / step time, FP64, k = 32"},
+           "results": res}
     print(json.dumps(out), flush=True)
 
 
@@ -641,12 +744,11 @@ def main_reference(a, rank, ws, W):
     et, snnz, info = reference_time(wl["row"], wl["col"], wl["val"], wl["x"], a.format, 0.0,
                                     calls=a.steps, row_frac=frac, warm=W)
     value = 2.0 * snnz / et / 1e9
-    fmt_name = {"CSR": "CSR"}.get(a.format, a.format)
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps,
            "warmup": W, "ms_per_step": et * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64", "data": f"synthetic: {wl['desc']}",
-           "config": {"workload": wl["name"], "format": fmt_name, "n": n, "nnz": nnz,
-                      "parallelism": "host OpenMP"},
+           "config": run_config(wl, format_name(a.format), "f64", "u32", alg_bytes(n, nnz)),
+           "kernel": {"family": "reference CPU", "name": info["kernel"], "threads": info["cores"]},
            "cpu_baseline": {"value": value, "unit": UNIT, "cores": info["cores"], "kind": "reference",
                             "sample": f"{info['kernel']} (intSpmv_main.c) on the first {info['rows']} rows "
                                       f"({snnz} nonzeros) of the workload per step, {info['cores']} threads"},

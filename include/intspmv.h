@@ -35,11 +35,32 @@ extern "C" {
 #endif
 
 /* ---------------------------------------------------------------------------
- * Compile-time configuration of the reference (M:51-109, ic.sh:43).  Only the
- * FP_TYPE=FP_DOUBLE build of the reference works (M:207 typo, `_pd`
- * intrinsics), so FPT is double.
+ * Compile-time configuration of the reference (M:51-109, ic.sh:43).  FPT is
+ * the value type, chosen as the reference chooses it: FP_TYPE=FP_DOUBLE (the
+ * default) or FP_TYPE=FP_FLOAT on the compile line (or ISPMV_FPT_FLOAT).
+ * The reference's own FP32 build does not compile (the M:207 typo, `_pd`
+ * intrinsics); here it does.  With FPT = float the structs hold float
+ * values and the layer-1 and layer-2 names below resolve to their `_f32`
+ * symbols (the same library exports both): values, x and y are FP32, every
+ * product and sum is computed in FP64 and y is rounded to FP32 once.  The
+ * device plans (layer 3) and the GPU format builders are FP64 only.
  * ------------------------------------------------------------------------ */
-typedef double FPT;        /* M:63-73 */
+#ifndef FP_FLOAT
+#define FP_FLOAT 1  /* M:51-53 */
+#endif
+#ifndef FP_DOUBLE
+#define FP_DOUBLE 2 /* M:57-59 */
+#endif
+#if defined(FP_TYPE) && !defined(ISPMV_FPT_FLOAT)
+#if FP_TYPE == FP_FLOAT
+#define ISPMV_FPT_FLOAT 1
+#endif
+#endif
+#ifdef ISPMV_FPT_FLOAT
+typedef float FPT;         /* M:63-66 */
+#else
+typedef double FPT;        /* M:70-73 */
+#endif
 typedef unsigned int UIN;  /* M:77-79 */
 #define ISPMV_HBRICK_SIZE 8u /* M:101-103: brick / tile width */
 #define ISPMV_CHUNK_SIZE 8u  /* M:107-109: K1 chunk height */
@@ -52,6 +73,56 @@ typedef unsigned int UIN;  /* M:77-79 */
 #define ISPMV_ERR_TIMEOUT 4     /* a bounded device wait gave up */
 #define ISPMV_ERR_UNSUPPORTED 5 /* valid for the reference, not implemented */
 #define ISPMV_ERR_OVERFLOW 6    /* a u32 length or index would overflow */
+
+#ifdef ISPMV_FPT_FLOAT
+/* FPT = float: every function whose arguments hold FPT resolves to its FP32
+ * symbol. */
+#define ispmv_csr_stats ispmv_csr_stats_f32
+#define printMatrixStats printMatrixStats_f32
+#define ispmv_matrix_read ispmv_matrix_read_f32
+#define matrixReading matrixReading_f32
+#define ispmv_matrix_write ispmv_matrix_write_f32
+#define ispmv_csr_free ispmv_csr_free_f32
+#define ispmv_build_csr ispmv_build_csr_f32
+#define getFormatDataCSR getFormatDataCSR_f32
+#define ispmv_build_axc ispmv_build_axc_f32
+#define getFormatDataAXC getFormatDataAXC_f32
+#define ispmv_build_k1 ispmv_build_k1_f32
+#define getFormatDataK1 getFormatDataK1_f32
+#define ispmv_build_axt ispmv_build_axt_f32
+#define getFormatDataAXT getFormatDataAXT_f32
+#define ispmv_build_axc_cols ispmv_build_axc_cols_f32
+#define ispmv_build_axt_cols ispmv_build_axt_cols_f32
+#define ispmv_free_axc ispmv_free_axc_f32
+#define ispmv_free_k1 ispmv_free_k1_f32
+#define ispmv_free_axt ispmv_free_axt_f32
+#define getErrors getErrors_f32
+#define initVec initVec_f32
+#define fill_array fill_array_f32
+#define ispmv_dev_cf_csr ispmv_dev_cf_csr_f32
+#define ispmv_dev_int_axc ispmv_dev_int_axc_f32
+#define ispmv_dev_int_k1 ispmv_dev_int_k1_f32
+#define ispmv_dev_order_k1 ispmv_dev_order_k1_f32
+#define ispmv_dev_int_k1p ispmv_dev_int_k1p_f32
+#define ispmv_dev_int_axt_noc_h1 ispmv_dev_int_axt_noc_h1_f32
+#define ispmv_dev_int_axt_noc ispmv_dev_int_axt_noc_f32
+#define ispmv_dev_int_axt_com_h1 ispmv_dev_int_axt_com_h1_f32
+#define cf_CSR cf_CSR_f32
+#define int_axc int_axc_f32
+#define int_k1 int_k1_f32
+#define orderArrayK1 orderArrayK1_f32
+#define int_k1p int_k1p_f32
+#define int_axt_noc_h1 int_axt_noc_h1_f32
+#define int_axt_noc int_axt_noc_f32
+#define int_axt_com_h1 int_axt_com_h1_f32
+#define test_cf_CSR test_cf_CSR_f32
+#define test_int_AXC test_int_AXC_f32
+#define test_int_k1 test_int_k1_f32
+#define test_int_k1p test_int_k1p_f32
+#define test_int_axt_noc_h1 test_int_axt_noc_h1_f32
+#define test_int_axt_noc test_int_axt_noc_f32
+#define test_int_axt_com_h1 test_int_axt_com_h1_f32
+#endif
 
 /* ---------------------------------------------------------------------------
  * Reference structs, field for field (same order, same types).
@@ -156,6 +227,7 @@ str_formatData getFormatDataAXT(const UIN ompNT, const UIN bs, const UIN thw, co
 int ispmv_build_axc_cols(UIN ompNT, const str_matCSR *csr, const str_matAXC *axc, UIN **axi);
 int ispmv_build_axt_cols(UIN ompNT, const str_matCSR *csr, const str_matAXT *axt, UIN **axi);
 
+#ifndef ISPMV_FPT_FLOAT
 /* Block-diagonal CSR of `count` square matrices (no reference counterpart:
  * the batched path).  Matrix m's rows and columns start at off[m]; off has
  * count+1 entries.  Arrays are malloc'd (ispmv_csr_free); rl and the
@@ -169,6 +241,7 @@ int ispmv_csr_blockdiag(UIN count, const str_matCSR *mats, str_matCSR *out, UIN 
  * (ispmv_csr_free); rl and statistics filled.  Deterministic in (n, seed,
  * rl_lo, rl_hi, band) whatever the thread count. */
 int ispmv_gen_banded(UIN n, uint64_t seed, UIN rl_lo, UIN rl_hi, UIN band, str_matCSR *out);
+#endif
 
 /* Frees the arrays a builder allocated and zeroes the struct. */
 void ispmv_free_axc(str_matAXC *m);
@@ -179,6 +252,8 @@ void ispmv_free_axt(str_matAXT *m);
  * max_i |ref_i|, pos = first argmax. */
 void getErrors(const UIN len, const FPT *ar, const FPT *ac, str_err *sErr);
 void initVec(const UIN len, FPT *vec); /* M:361-367: vec[i] = i */
+/* fill_array, M:371-378: array[i] = val (host memory, ompNT threads). */
+void fill_array(const UIN ompNT, const UIN len, FPT val, FPT *array);
 
 /* ---------------------------------------------------------------------------
  * Layer 2a: kernels on DEVICE pointers (stream-ordered; `stream` is a
@@ -227,8 +302,10 @@ int ispmv_dev_int_axt_com_h1(UIN bn, UIN bs, UIN log, UIN thw, UIN tn, UIN lenAX
  * threads) race and must be serialised by the caller.  Nothing needs
  * clearing between calls: every call writes the part of the array it reads. */
 #define ISPMV_K1_NOALLOC_MAX_ROWS (1u << 20)
+#ifndef ISPMV_FPT_FLOAT
 int ispmv_dev_k1_spmv_noalloc(UIN nrows, UIN chunkNum, const FPT *val, const UIN *col, const UIN *chp,
                               const UIN *nmc, const UIN *permi, const FPT *vec, FPT *y, void *stream);
+#endif
 
 /* ---------------------------------------------------------------------------
  * Layer 2b: the reference's kernels by name on HOST pointers.  Each call
@@ -253,6 +330,33 @@ void int_axt_com_h1(const UIN ompNT, const UIN bn, const UIN bs, const UIN log, 
                     const UIN tn, const UIN lenAX, const UIN lenRWP, const FPT *ax,
                     const UIN *rwp, FPT *y);                                    /* M:1517 */
 
+/* ---------------------------------------------------------------------------
+ * Layer 2c: the reference's per-kernel harness (test_*, M:433-1609), as a
+ * reference caller times and checks kernels.  Each uploads its arrays to
+ * the GPU once, runs the kernel NUM_ITE times (AXT kernels on a y zeroed
+ * before every run, outside the timed region, as fill_array does, M:1420),
+ * and fills str_res: name (the reference's string), et = mean time of one
+ * kernel run in seconds (CUDA events around the launch on the GPU),
+ * ot = mean time of the reorder pass (test_int_k1 only: orderArrayK1, M:1001)
+ * else 0, flops = 2*nnz / et, and sErr = getErrors(nrows, ref, result).
+ * The arrays are those the reference-named builders produce.  Errors print
+ * and exit like the reference.
+ * ------------------------------------------------------------------------ */
+#define ISPMV_NUM_ITE_DEFAULT 250u /* M:93-95 */
+/* Runs per test_* call: $ISPMV_NUM_ITE when set, else ISPMV_NUM_ITE_DEFAULT;
+ * ispmv_set_num_ite(n) overrides both (0 restores them). */
+void ispmv_set_num_ite(UIN n);
+UIN ispmv_get_num_ite(void);
+str_res test_cf_CSR(const str_matCSR matCSR, const FPT *vec, const FPT *ref);            /* M:433 */
+str_res test_int_AXC(const UIN ompNT, const str_matAXC matAXC, const FPT *ref);          /* M:736 */
+str_res test_int_k1(const UIN ompNT, const str_matK1 matK1, const FPT *vec, const FPT *ref); /* M:980 */
+str_res test_int_k1p(const UIN ompNT, const str_matK1 matK1, const FPT *vec, const FPT *ref); /* M:1070 */
+str_res test_int_axt_noc_h1(const UIN ompNT, const str_matAXT matAXT, const FPT *ref);   /* M:1408 */
+str_res test_int_axt_noc(const UIN ompNT, const str_matAXT matAXT, const FPT *ref);      /* M:1478 */
+str_res test_int_axt_com_h1(const UIN ompNT, const UIN bs, const str_matAXT matAXT,
+                            const FPT *ref);                                             /* M:1570 */
+
+#ifndef ISPMV_FPT_FLOAT
 /* Format conversion on the GPU (no reference counterpart: the reference
  * converts on the host, getFormatDataAXT M:1275-1381).  Builds the same
  * con/ax/sec arrays as getFormatDataAXT, bit for bit, from a CSR matrix and
@@ -406,6 +510,8 @@ typedef struct {
   char name[32];
 } ispmv_plan_info;
 int ispmv_plan_get_info(ispmv_plan p, ispmv_plan_info *info);
+
+#endif /* !ISPMV_FPT_FLOAT: GPU format builders and plans are FP64 */
 
 /* Library facts and diagnostics. */
 const char *ispmv_version(void);

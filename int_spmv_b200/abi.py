@@ -108,6 +108,17 @@ PROTOTYPES: dict[str, tuple] = {
     "ispmv_free_axt": (None, [P_AXT]),
     "getErrors": (None, [UIN, P_FPT, P_FPT, C.POINTER(StrErr)]),
     "initVec": (None, [UIN, P_FPT]),
+    "fill_array": (None, [UIN, UIN, C.c_double, P_FPT]),
+    # the reference's per-kernel harness (test_*), runs per call
+    "ispmv_set_num_ite": (None, [UIN]),
+    "ispmv_get_num_ite": (UIN, []),
+    "test_cf_CSR": (StrRes, [StrMatCSR, P_FPT, P_FPT]),
+    "test_int_AXC": (StrRes, [UIN, StrMatAXC, P_FPT]),
+    "test_int_k1": (StrRes, [UIN, StrMatK1, P_FPT, P_FPT]),
+    "test_int_k1p": (StrRes, [UIN, StrMatK1, P_FPT, P_FPT]),
+    "test_int_axt_noc_h1": (StrRes, [UIN, StrMatAXT, P_FPT]),
+    "test_int_axt_noc": (StrRes, [UIN, StrMatAXT, P_FPT]),
+    "test_int_axt_com_h1": (StrRes, [UIN, UIN, StrMatAXT, P_FPT]),
     # device kernels on device pointers
     "ispmv_dev_cf_csr": (C.c_int, [UIN, VP, VP, VP, VP, VP, VP]),
     "ispmv_dev_int_axc": (C.c_int, [UIN, VP, VP, VP, VP]),

@@ -40,8 +40,18 @@ def _nvcc() -> str:
     raise RuntimeError("nvcc not found: the CUDA toolkit is required to build int_spmv_b200")
 
 
+# Sources compiled a second time with FPT = float (-DISPMV_FPT_FLOAT): the
+# reference's API in its FP_TYPE=FP_FLOAT configuration, `_f32` symbols.
+F32_SOURCES = ("builders.c", "io.c", "literal.cu", "harness.cu")
+
+
 def sources() -> list[Path]:
     return sorted((CSRC / "host").glob("*.c")) + sorted((CSRC / "cuda").glob("*.cu"))
+
+
+def units() -> list[tuple[Path, bool]]:
+    """(source, FPT = float) for every object of the library."""
+    return [(p, False) for p in sources()] + [(p, True) for p in sources() if p.name in F32_SOURCES]
 
 
 def _deps() -> list[Path]:
@@ -69,12 +79,14 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     OBJ.mkdir(exist_ok=True)
     nvcc, cc = _nvcc(), _cc()
     objs = []
-    for src in sources():
-        obj = OBJ / (src.stem + (".c.o" if src.suffix == ".c" else ".cu.o"))
+    for src, f32 in units():
+        obj = OBJ / (src.stem + ("_f32" if f32 else "") + (".c.o" if src.suffix == ".c" else ".cu.o"))
+        defs = ["-DISPMV_FPT_FLOAT"] if f32 else []
         if src.suffix == ".c":
-            cmd = [cc, *CC_FLAGS, f"-I{INCLUDE}", "-c", str(src), "-o", str(obj)]
+            cmd = [cc, *CC_FLAGS, *defs, f"-I{INCLUDE}", "-c", str(src), "-o", str(obj)]
         else:
-            cmd = [nvcc, *ARCH, *NVCC_FLAGS, f"-I{INCLUDE}", f"-I{CSRC / 'cuda'}", "-c", str(src), "-o", str(obj)]
+            cmd = [nvcc, *ARCH, *NVCC_FLAGS, *defs, f"-I{INCLUDE}", f"-I{CSRC / 'cuda'}", "-c", str(src), "-o",
+                   str(obj)]
         if verbose:
             print(" ".join(cmd))
         _run(cmd)

@@ -23,6 +23,12 @@
 //                   segment, so row-0 segments whose descriptor is 0 are
 //                   summed (the reference skips them, M:1555) and segment
 //                   sums are true sums, not prefix differences (M:1559).
+//
+// The file is compiled twice: with FPT = double (the reference's FP_DOUBLE
+// build) and with ISPMV_FPT_FLOAT (FPT = float, every exported name gets
+// the `_f32` suffix through intspmv.h).  Products and sums are FP64 in both;
+// an FP32 result is rounded once when it is stored (or, for the AXT kernels,
+// when each row run is added to y).
 #include <cuda.h>
 
 #include <cstdio>
@@ -47,12 +53,12 @@ __global__ void __launch_bounds__(TPB) k_cf_csr(UIN n, const UIN *__restrict__ r
   double s = 0.0;
   if (live) {
     const UIN b = row[r], e = row[r + 1];
-    for (UIN j = b + lane8; j < e; j += 8) s = fma(ld_stream(val + j), ldg(x + ld_stream(col + j)), s);
+    for (UIN j = b + lane8; j < e; j += 8) s = fma((double)ld_stream(val + j), (double)ldg(x + ld_stream(col + j)), s);
   }
   s += __shfl_xor_sync(FULL, s, 4);
   s += __shfl_xor_sync(FULL, s, 2);
   s += __shfl_xor_sync(FULL, s, 1);
-  if (live && lane8 == 0) y[r] = s;
+  if (live && lane8 == 0) y[r] = (FPT)s;
 }
 
 __global__ void __launch_bounds__(TPB) k_axc(UIN n, const FPT *__restrict__ ax,
@@ -63,12 +69,12 @@ __global__ void __launch_bounds__(TPB) k_axc(UIN n, const FPT *__restrict__ ax,
   double s = 0.0;
   if (live) {
     const UIN b = brp[r], e = brp[r + 1];
-    for (UIN p = b; p < e; p += 16) s = fma(ld_stream(ax + p + lane8), ld_stream(ax + p + 8 + lane8), s);
+    for (UIN p = b; p < e; p += 16) s = fma((double)ld_stream(ax + p + lane8), (double)ld_stream(ax + p + 8 + lane8), s);
   }
   s += __shfl_xor_sync(FULL, s, 4);
   s += __shfl_xor_sync(FULL, s, 2);
   s += __shfl_xor_sync(FULL, s, 1);
-  if (live && lane8 == 0) y[r] = s;
+  if (live && lane8 == 0) y[r] = (FPT)s;
 }
 
 // K1 (M:943-965) and K1 with integrated reordering (M:1026-1066).
@@ -84,13 +90,13 @@ __global__ void __launch_bounds__(TPB) k_k1(UIN chunkNum, unsigned char mask, co
   double s = 0.0;
   for (UIN k = 0; k < m; k++) {
     const size_t p = (size_t)off + (size_t)k * 8 + lane8;
-    s = fma(ld_stream(val + p), ldg(x + ld_stream(col + p)), s);
+    s = fma((double)ld_stream(val + p), (double)ldg(x + ld_stream(col + p)), s);
   }
   if (!SCATTER) {
-    res[c * 8 + lane8] = s;
+    res[c * 8 + lane8] = (FPT)s;
   } else {
     const bool last = (c + 1 == chunkNum);
-    if (!last || ((mask >> lane8) & 1u)) res[permi[c * 8 + lane8]] = s;
+    if (!last || ((mask >> lane8) & 1u)) res[permi[c * 8 + lane8]] = (FPT)s;
   }
 }
 
@@ -117,7 +123,7 @@ __global__ void __launch_bounds__(TPB) k_axt_noc_h1(UIN tileNum, const FPT *__re
     double p = 0.0;
     UIN r = NO_ROW;
     if (live) {
-      p = ld_stream(ax + t * 16 + lane8) * ld_stream(ax + t * 16 + 8 + lane8);
+      p = (double)ld_stream(ax + t * 16 + lane8) * (double)ld_stream(ax + t * 16 + 8 + lane8);
       r = rwp[t];
     }
     // within-tile sum (lane8 == 0 holds it)
@@ -129,15 +135,15 @@ __global__ void __launch_bounds__(TPB) k_axt_noc_h1(UIN tileNum, const FPT *__re
     const bool head = (lane == 0) ? (r != crow) : (r != rprev);
     if (lane == 0) {
       if (!head) p += csum;
-      else if (crow != NO_ROW) atomicAdd(y + crow, csum);  // the carried run ended last step
+      else if (crow != NO_ROW) atomicAdd(y + crow, (FPT)csum);  // the carried run ended last step
     }
     const double s = warp_seg_scan(p, head);
     const UIN rnext = __shfl_down_sync(FULL, r, 1);
-    if (lane < 31 && r != rnext && r != NO_ROW) atomicAdd(y + r, s);
+    if (lane < 31 && r != rnext && r != NO_ROW) atomicAdd(y + r, (FPT)s);
     crow = __shfl_sync(FULL, r, 31);
     csum = __shfl_sync(FULL, s, 31);
   }
-  if (lane == 0 && crow != NO_ROW) atomicAdd(y + crow, csum);
+  if (lane == 0 && crow != NO_ROW) atomicAdd(y + crow, (FPT)csum);
 }
 
 // AXT NOC tileH>1 (M:1443-1474): one warp per tile.
@@ -148,7 +154,8 @@ __global__ void __launch_bounds__(TPB) k_axt_noc(UIN tileNum, UIN th, const FPT 
   if (t >= tileNum) return;
   const FPT *tile = ax + t * (size_t)th * 16;
   double s = 0.0;
-  for (UIN R = lane >> 3; R < th; R += 4) s = fma(ld_stream(tile + R * 16 + c), ld_stream(tile + R * 16 + 8 + c), s);
+  for (UIN R = lane >> 3; R < th; R += 4)
+    s = fma((double)ld_stream(tile + R * 16 + c), (double)ld_stream(tile + R * 16 + 8 + c), s);
   s += __shfl_xor_sync(FULL, s, 8);
   s += __shfl_xor_sync(FULL, s, 16);
   // lanes 0..7 hold the 8 column sums; combine runs of equal rows
@@ -157,7 +164,7 @@ __global__ void __launch_bounds__(TPB) k_axt_noc(UIN tileNum, UIN th, const FPT 
   const bool head = (lane == 0) || (r != rprev);
   const double v = warp_seg_scan(lane < 8 ? s : 0.0, head);
   const UIN rnext = __shfl_down_sync(FULL, r, 1);
-  if (lane < 8 && r != rnext) atomicAdd(y + r, v);
+  if (lane < 8 && r != rnext) atomicAdd(y + r, (FPT)v);
 }
 
 // AXT COM tileH=1 (M:1517-1566), true segmented sums.
@@ -178,7 +185,7 @@ __global__ void __launch_bounds__(TPB) k_axt_com_h1(UIN bs, UIN lg, UIN lenRWP, 
     UIN hrow = 0;
     if (live) {
       const size_t a = (p >> 3) * 16 + (p & 7);
-      v = ld_stream(ax + a) * ld_stream(ax + a + 8);
+      v = (double)ld_stream(ax + a) * (double)ld_stream(ax + a + 8);
       const UIN d = rwp[p];
       head = (d != 0) || ((p & (bs - 1)) == 0);
       hrow = d >> lg;
@@ -195,15 +202,15 @@ __global__ void __launch_bounds__(TPB) k_axt_com_h1(UIN bs, UIN lg, UIN lenRWP, 
     const bool seg = (lane == 0) ? (head || r != crow) : (head || !live);
     if (lane == 0) {
       if (!seg) v += csum;
-      else if (crow != NO_ROW) atomicAdd(y + crow, csum);  // the carried run ended last step
+      else if (crow != NO_ROW) atomicAdd(y + crow, (FPT)csum);  // the carried run ended last step
     }
     const double s = warp_seg_scan(v, seg);
     const bool nexthead = __shfl_down_sync(FULL, (unsigned)(head || !live), 1) != 0;
-    if (lane < 31 && live && nexthead && r != NO_ROW) atomicAdd(y + r, s);
+    if (lane < 31 && live && nexthead && r != NO_ROW) atomicAdd(y + r, (FPT)s);
     crow = __shfl_sync(FULL, r, 31);
     csum = __shfl_sync(FULL, s, 31);
   }
-  if (lane == 0 && crow != NO_ROW) atomicAdd(y + crow, csum);
+  if (lane == 0 && crow != NO_ROW) atomicAdd(y + crow, (FPT)csum);
 }
 
 inline unsigned blocks_for(size_t threads) { return (unsigned)((threads + TPB - 1) / TPB); }
@@ -283,6 +290,7 @@ ISPMV_API int ispmv_dev_int_axt_com_h1(UIN bn, UIN bs, UIN log, UIN thw, UIN tn,
   return check_launch("ispmv_dev_int_axt_com_h1");
 }
 
+#ifndef ISPMV_FPT_FLOAT  // FP64 only
 // ---------------------------------------------------------------------------
 // K1 product in original row order that allocates nothing.  The chunk-order
 // result of the K1 kernel (the `res` array int_k1 hands to orderArrayK1)
@@ -379,6 +387,8 @@ ISPMV_API int ispmv_dev_k1_spmv_noalloc(UIN nrows, UIN chunkNum, const FPT *val,
   lit::k_order<<<lit::blocks_for(nrows), lit::TPB, 0, as_stream(stream)>>>(nrows, permi, res, y);
   return check_launch("ispmv_dev_k1_spmv_noalloc (reorder)");
 }
+
+#endif  // !ISPMV_FPT_FLOAT
 
 // ---------------------------------------------------------------------------
 // Host-pointer forms with the reference's names.  A small grow-only pool of

@@ -478,6 +478,13 @@ API void initVec(const UIN len, FPT *vec) {
   for (UIN i = 0; i < len; i++) vec[i] = (FPT)i;
 }
 
+/* fill_array, M:371-378: array[i] = val on ompNT threads (0: all). */
+API void fill_array(const UIN ompNT, const UIN len, FPT val, FPT *array) {
+  const int nt = nthreads(ompNT);
+#pragma omp parallel for num_threads(nt) schedule(static)
+  for (long long i = 0; i < (long long)len; i++) array[i] = val;
+}
+
 /* --------------------------------------- compat (exit-on-error) forms -- */
 static void die(const char *fn, int st) {
   fflush(stdout);
@@ -515,6 +522,7 @@ API str_formatData getFormatDataAXT(const UIN ompNT, const UIN bs, const UIN thw
   return fd;
 }
 
+#ifndef ISPMV_FPT_FLOAT /* the batched path is FP64 */
 /* ------------------------------------------------- batched matrices -- */
 /* Block-diagonal CSR of `count` square matrices: matrix m's rows and columns
  * start at off[m] (off has count+1 entries).  Arrays are malloc'd (free with
@@ -558,3 +566,4 @@ API int ispmv_csr_blockdiag(UIN count, const str_matCSR *mats, str_matCSR *out, 
   }
   return ispmv_csr_stats(out);
 }
+#endif
