@@ -42,6 +42,10 @@ SPMV_CANDIDATES = [
     ("COM128", dict(kernel="wide", variant=26)),  # 8 slots per lane, per-CTA x window by one bulk copy
     ("COM128", dict(kernel="wide", variant=32)),  # 8 slots per lane, next batch's columns loaded ahead
     ("NOC1", dict(kernel="wide", variant=0)),
+    ("NOC4", dict()),                             # tile columns as a lane-interleaved stream (AUTO variant)
+    ("NOC8", dict()),
+    ("CSR", dict()),                              # CSR order as a lane-interleaved stream (AUTO variant)
+    ("AXC", dict()),                              # the brick stream, lane-interleaved (AUTO variant)
     ("COM128", dict(kernel="ldg", variant=0)),
     ("COM128", dict(kernel="ldg", variant=2)),
     ("COM128", dict(kernel="ldg", variant=12)),
@@ -56,7 +60,8 @@ SPMV_CANDIDATES = [
     ("K1P", dict()),
 ]
 SPMM_CANDIDATES = [("COM128", dict(kernel="ldg", rhs_block=b)) for b in (8, 16, 32)] + \
-                  [("NOC1", dict(kernel="ldg", rhs_block=b)) for b in (8, 16, 32)]
+                  [("NOC1", dict(kernel="ldg", rhs_block=b)) for b in (8, 16, 32)] + \
+                  [("COM128", dict(kernel="wide", variant=4, rhs_block=b)) for b in (8, 16, 32)]
 
 
 def cache_path() -> Path:

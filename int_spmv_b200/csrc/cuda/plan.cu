@@ -78,6 +78,7 @@ struct ispmv_plan_s {
   UIN *mm_row = nullptr;             // SpMM records (allocated on first use)
   double *mm_sum = nullptr;
   size_t mm_cap = 0;                 // doubles in mm_sum
+  size_t mm_rows_cap = 0;            // entries of mm_row
   std::vector<void *> owned;
   ispmv_plan_info info{};
   std::vector<cudaEvent_t> tev;      // kernel timing: event pairs around the main kernel (a ring)
@@ -360,6 +361,24 @@ double random_far_fraction(const str_matCSR *csr) {
     far += !near_next;
   }
   return (double)far / (double)S;
+}
+
+// AUTO on a slot-stream plan: the lane-interleaved kernel (stream_wide) and
+// its variant.  8 slots per lane for rows of fewer than 16 nonzeros on
+// average, with per-CTA x windows where the columns are scattered (FP64
+// values) or the next batch's columns loaded ahead (FP32 values, whose
+// kernel has the registers for it); else 16 slots per lane, bulk-copy staged
+// for FP64 values with u32 columns that are not scattered (measured fastest
+// there), plain loads for scattered columns and for the FP32, lo-word and
+// 16-bit-delta forms.  An explicit variant is kept.
+void auto_wide(ispmv_plan_s *p, const str_matCSR *csr) {
+  p->opts.kernel = ISPMV_KERNEL_WIDE;
+  if (p->opts.variant != 0) return;
+  const bool long_rows = (double)csr->nnz >= 16.0 * (double)p->n;
+  const bool plain = p->opts.val_kind == ISPMV_VAL_F64 && p->opts.col_kind == ISPMV_COL_U32;
+  const bool scattered = random_far_fraction(csr) >= 0.05;
+  const int short_scattered = p->opts.val_kind == ISPMV_VAL_F32 ? 32 : 26;
+  p->opts.variant = !long_rows ? (scattered && !narrow_kinds(p) ? short_scattered : 4) : plain && !scattered ? 11 : 0;
 }
 
 // The per-CTA x windows of the staged stream_wide variants: CTA t walks
@@ -656,8 +675,8 @@ ISPMV_API int ispmv_plan_csr(const str_matCSR *csr, const ispmv_plan_opts *o, is
   p->nnz = csr->nnz;
   p->slots = csr->nnz;
   int st = ISPMV_OK;
-  if (narrow_kinds(p) && p->opts.kernel == ISPMV_KERNEL_AUTO) p->opts.kernel = ISPMV_KERNEL_LDG;
-  if (p->opts.kernel == ISPMV_KERNEL_AUTO || p->opts.kernel == ISPMV_KERNEL_ROWS) {
+  if (p->opts.kernel == ISPMV_KERNEL_AUTO) auto_wide(p, csr);  // the CSR-order slot stream
+  if (p->opts.kernel == ISPMV_KERNEL_ROWS) {
     // the naive CSR product on the GPU: L lanes per row
     if (narrow_kinds(p)) { ispmv_plan_destroy(p); return ISPMV_ERR_UNSUPPORTED; }
     p->opts.kernel = ISPMV_KERNEL_ROWS;
@@ -1089,8 +1108,8 @@ ISPMV_API int ispmv_plan_axc(const str_matCSR *csr, const str_matAXC *axc, const
   std::vector<UIN> c(axi, axi + p->slots);
   for (size_t s = 0; s < p->slots; s++) v[s] = axc->ax[(s / 8) * 16 + s % 8];
   int st = ISPMV_OK;
-  if (narrow_kinds(p) && p->opts.kernel == ISPMV_KERNEL_AUTO) p->opts.kernel = ISPMV_KERNEL_LDG;
-  if (p->opts.kernel == ISPMV_KERNEL_AUTO || p->opts.kernel == ISPMV_KERNEL_ROWS) {
+  if (p->opts.kernel == ISPMV_KERNEL_AUTO) auto_wide(p, csr);  // the brick stream
+  if (p->opts.kernel == ISPMV_KERNEL_ROWS) {
     // the reference's row loop (M:711-732): 8 lanes per row over its bricks
     if (narrow_kinds(p)) { ispmv_plan_destroy(p); return ISPMV_ERR_UNSUPPORTED; }
     p->opts.kernel = ISPMV_KERNEL_ROWS;
@@ -1170,15 +1189,35 @@ ISPMV_API int ispmv_plan_axt(const str_matCSR *csr, const str_matAXT *axt, const
   } else {
     snprintf(name, sizeof name, "AXT_NOC_H%u", th);
   }
-  if (com || th == 1) {
+  // tileH > 1 on the slot-stream kernels: the tiles' slots in tile-column
+  // order (tile, column, sub-row), where each row is one contiguous run
+  const bool noc_stream = !com && th > 1 && (p->opts.kernel == ISPMV_KERNEL_AUTO || p->opts.kernel == ISPMV_KERNEL_WIDE);
+  if (com || th == 1 || noc_stream) {
     // the tileH=1 tile stream and the packed compacted stream: every row is
-    // a contiguous run of slots starting at the slot its con[] names
+    // a contiguous run of slots starting at the slot its con[] names; a
+    // tileH > 1 tile (th sub-rows of 8 columns, a row filling columns top to
+    // bottom, M:1188-1221) read column by column is such a stream too
     p->slots = com ? csr->nnz : (size_t)axt->lenAX / 2;
     std::vector<double> v(p->slots);
-    std::vector<UIN> c(axi, axi + p->slots);
-    for (size_t q = 0; q < p->slots; q++) v[q] = axt->ax[(q / 8) * 16 + q % 8];
+    std::vector<UIN> c(p->slots);
     std::vector<size_t> start(p->n);
-    for (UIN r = 0; r < p->n; r++) start[r] = (size_t)(axt->con[r] / 16) * 8 + axt->con[r] % 16;
+    if (th == 1) {
+      std::copy(axi, axi + p->slots, c.begin());
+      for (size_t q = 0; q < p->slots; q++) v[q] = axt->ax[(q / 8) * 16 + q % 8];
+      for (UIN r = 0; r < p->n; r++) start[r] = (size_t)(axt->con[r] / 16) * 8 + axt->con[r] % 16;
+    } else {
+      const size_t tile = (size_t)8 * th;  // value slots per tile
+      for (size_t q = 0; q < p->slots; q++) {  // q: slot in ax order (tile, sub-row, column)
+        const size_t T = q / tile, R = (q % tile) / 8, C = q % 8;
+        const size_t sc = T * tile + C * th + R;  // the same slot in column order
+        v[sc] = axt->ax[(q / 8) * 16 + q % 8];
+        c[sc] = axi[q];
+      }
+      for (UIN r = 0; r < p->n; r++) {  // con = T*16*th + R*16 + C (M:1118-1148)
+        const size_t T = axt->con[r] / (16 * th), rem = axt->con[r] % (16 * th);
+        start[r] = T * tile + (rem % 16) * th + rem / 16;
+      }
+    }
     if (p->opts.kernel == ISPMV_KERNEL_AUTO) {
       // the lane-interleaved kernel: 8 slots per lane for rows of fewer than
       // 16 nonzeros on average, where the columns are scattered with per-CTA
@@ -1187,15 +1226,7 @@ ISPMV_API int ispmv_plan_axt(const str_matCSR *csr, const str_matAXT *axt, const
       // bulk-copy staged for FP64 values with u32 columns that are not
       // scattered (measured fastest there), plain loads for scattered columns
       // and for the FP32, lo-word and 16-bit-delta forms
-      p->opts.kernel = ISPMV_KERNEL_WIDE;
-      if (p->opts.variant == 0) {
-        const bool long_rows = (double)csr->nnz >= 16.0 * (double)p->n;
-        const bool plain = p->opts.val_kind == ISPMV_VAL_F64 && p->opts.col_kind == ISPMV_COL_U32;
-        const bool scattered = random_far_fraction(csr) >= 0.05;
-        const int short_scattered = p->opts.val_kind == ISPMV_VAL_F32 ? 32 : 26;
-        p->opts.variant = !long_rows ? (scattered && !narrow_kinds(p) ? short_scattered : 4)
-                                     : plain && !scattered ? 11 : 0;
-      }
+      auto_wide(p, csr);
     }
     st = setup_stream(p, csr, v, c, start);
   } else {
@@ -1798,37 +1829,44 @@ bool tmem_plan(const ispmv_plan_s *p) {
   return p->opts.kernel == ISPMV_KERNEL_WIDE && wide_variant(p->opts.variant).tmem;
 }
 
-template <int G, typename VT>
+// One pass per block of CB = G*W right-hand sides (G lanes per group, W
+// columns per lane).
+template <int G, int W, typename VT>
 int spmm_blocks(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
-  constexpr int NG = 32 / G;
+  constexpr int NG = 32 / G, CB = G * W;
   const size_t nparts = p->nseg * NG, nrec = 2 * nparts;
-  if (!p->mm_row) TRY(dev_alloc(p, std::max<size_t>(1, nrec), &p->mm_row));
-  if (p->mm_cap < nrec * G) {
-    TRY(dev_alloc(p, std::max<size_t>(1, nrec * G), &p->mm_sum));
-    p->mm_cap = nrec * G;
+  if (p->mm_rows_cap < nrec) {
+    TRY(dev_alloc(p, std::max<size_t>(1, nrec), &p->mm_row));
+    p->mm_rows_cap = nrec;
+  }
+  if (p->mm_cap < nrec * CB) {
+    TRY(dev_alloc(p, std::max<size_t>(1, nrec * CB), &p->mm_sum));
+    p->mm_cap = nrec * CB;
   }
   const VT *val = static_cast<const VT *>(p->val);
-  for (UIN j0 = 0; j0 < k; j0 += G) {
-    mm::Out o{Y, p->rowmap, p->mm_row, p->mm_sum, k, j0, std::min<UIN>(G, k - j0)};
+  for (UIN j0 = 0; j0 < k; j0 += CB) {
+    mm::Out o{Y, p->rowmap, p->mm_row, p->mm_sum, k, j0, std::min<UIN>(CB, k - j0)};
     const unsigned g = (unsigned)((p->nseg * 32 + 255) / 256);
-    mm::stream_spmm<G, VT><<<g, 256, 0, s>>>(p->slots, p->slots_pad, p->seg_slots, p->nseg, val, p->col, p->heads,
-                                             p->segh, X, o, il_spl(p));
+    mm::stream_spmm<G, W, VT><<<g, 256, 0, s>>>(p->slots, p->slots_pad, p->seg_slots, p->nseg, val, p->col,
+                                                p->heads, p->segh, X, o, il_spl(p));
     TRY(check_launch("stream_spmm"));
-    const size_t work = std::max(nrec, p->nempty) * G;
-    mm::spmm_fixup<G><<<(unsigned)((work + 255) / 256), 256, 0, s>>>(nrec, p->mm_row, p->mm_sum, p->empty,
-                                                                     p->nempty, o);
+    const size_t work = std::max(nrec, p->nempty) * CB;
+    mm::spmm_fixup<CB><<<(unsigned)((work + 255) / 256), 256, 0, s>>>(nrec, p->mm_row, p->mm_sum, p->empty,
+                                                                      p->nempty, o);
     TRY(check_launch("spmm_fixup"));
   }
   return ISPMV_OK;
 }
 
+// RHS block 8, 16 or 32 columns (ispmv_plan_opts.rhs_block, else by k): 4, 8
+// or 16 lanes per group with two columns per lane.
 template <typename VT>
 int spmm_run(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
   int g = p->opts.rhs_block;
   if (g != 8 && g != 16 && g != 32) g = k <= 8 ? 8 : k <= 16 ? 16 : 32;
-  if (g == 8) return spmm_blocks<8, VT>(p, k, X, Y, s);
-  if (g == 16) return spmm_blocks<16, VT>(p, k, X, Y, s);
-  return spmm_blocks<32, VT>(p, k, X, Y, s);
+  if (g == 8) return spmm_blocks<4, 2, VT>(p, k, X, Y, s);
+  if (g == 16) return spmm_blocks<8, 2, VT>(p, k, X, Y, s);
+  return spmm_blocks<16, 2, VT>(p, k, X, Y, s);
 }
 }  // namespace
 

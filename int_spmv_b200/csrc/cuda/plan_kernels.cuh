@@ -70,30 +70,51 @@ __global__ void __launch_bounds__(TPB) axc_rows(UIN n, const UIN *__restrict__ b
 }
 
 // ----------------------------------------------------------------- K1 --
-// 8 lanes per chunk; SCATTER writes y[permi] (K1 with integrated
-// reordering), else res in chunk order (then k1_order).
+// 8 lanes per chunk (lane = row of the chunk: each chunk column is one
+// coalesced 64-byte load); SCATTER writes y[permi] (K1 with integrated
+// reordering), else res in chunk order (then k1_order).  K1 orders rows by
+// length, so a chunk's rows are unrelated rows of the matrix and nearly
+// every gather misses the lines its neighbours touched: the column loop is
+// unrolled U = 8 deep with independent sums, so a lane's 8 value/column
+// loads and then its 8 gathers are in flight together.
 template <typename VT, bool SCATTER>
 __global__ void __launch_bounds__(TPB) k1_chunks(UIN n, UIN chunkNum, const UIN *__restrict__ chp,
                                                  const UIN *__restrict__ nmc, const UIN *__restrict__ permi,
                                                  const UIN *__restrict__ col, const VT *__restrict__ val,
                                                  const FPT *__restrict__ x, FPT *__restrict__ out, int beta) {
+  constexpr int U = 8;
   const unsigned lane8 = threadIdx.x & 7u;
   const size_t c = ((size_t)blockIdx.x * TPB + threadIdx.x) >> 3;
   if (c >= chunkNum) return;
   const size_t off = chp[c];
   const UIN m = nmc[c];
-  double s0 = 0.0, s1 = 0.0;
+  double acc[U];
+#pragma unroll
+  for (int u = 0; u < U; u++) acc[u] = 0.0;
   UIN k = 0;
-  for (; k + 1 < m; k += 2) {
+  for (; k + U <= m; k += U) {
     const size_t p = off + (size_t)k * 8 + lane8;
-    s0 = fmac<VT>(ld_stream(val + p), ldg(x + ld_stream(col + p)), s0);
-    s1 = fmac<VT>(ld_stream(val + p + 8), ldg(x + ld_stream(col + p + 8)), s1);
+    VT v[U];
+    UIN cc[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+      v[u] = ld_stream(val + p + 8 * u);
+      cc[u] = ld_stream(col + p + 8 * u);
+    }
+    double xv[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) xv[u] = ldg(x + cc[u]);
+#pragma unroll
+    for (int u = 0; u < U; u++) acc[u] = fmac<VT>(v[u], xv[u], acc[u]);
   }
-  if (k < m) {
-    const size_t p = off + (size_t)k * 8 + lane8;
-    s0 = fmac<VT>(ld_stream(val + p), ldg(x + ld_stream(col + p)), s0);
+#pragma unroll
+  for (int u = 0; u < U; u++) {  // the chunk's last m % U columns
+    if (k + u < m) {
+      const size_t p = off + (size_t)(k + u) * 8 + lane8;
+      acc[u] = fmac<VT>(ld_stream(val + p), ldg(x + ld_stream(col + p)), acc[u]);
+    }
   }
-  const double s = s0 + s1;
+  const double s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
   const size_t i = c * 8 + lane8;
   if (SCATTER) {
     if (i < n) {

@@ -1,12 +1,13 @@
 // spmm.cuh - multi-RHS SpMM on the slot stream: Y = A X, X and Y row-major
 // n x k (FP64), one plan's slot stream read once for all k right-hand sides.
 //
-// A warp splits into 32/G groups of G lanes; lane j of a group owns column
-// j0 + j of the current column block (G = 8, 16 or 32 columns).  Each group
-// walks its own contiguous part of the warp's segment slot by slot: 8 slots'
-// values and columns are loaded per step (one per lane, coalesced) and
-// broadcast with shuffles, each lane reads X[col*k + j0 + j] (the group reads
-// a contiguous row piece of X) and accumulates.  Row starts come from the
+// A warp splits into 32/G groups of G lanes; lane jl of a group owns the W
+// columns j0 + W*jl .. of the current column block (G*W = 8, 16 or 32
+// columns).  Each group walks its own contiguous part of the warp's segment:
+// G slots' values and columns are loaded per step (one per lane, coalesced)
+// and broadcast with shuffles, each lane reads its W-wide piece of row
+// X[col] (the group reads a contiguous row piece of X) and accumulates.
+// Row starts come from the
 // stream's bitmap; a row that ends inside the group's part is written to Y
 // directly, the runs open at the part's two ends become G-wide records that
 // spmm_fixup adds per row.  Deterministic, no atomics.  `il_spl` > 0 reads
@@ -28,13 +29,23 @@ struct Out {
 
 __device__ __forceinline__ UIN real_row(const Out &o, UIN r) { return o.rowmap ? o.rowmap[r] : r; }
 
-template <int G, typename VT>
+// G lanes per group, W (1 or 2) consecutive right-hand sides per lane: a
+// pass covers CB = G*W columns.  Per step the group loads G slots (one per
+// lane) and then works through them SUB at a time in two phases: first the
+// X rows of all SUB slots are loaded into registers (W-wide vector loads of
+// the group's contiguous piece of each row), then the row starts are
+// handled and the products accumulated.  The loads of a sub-batch are thus
+// in flight together, ahead of the stores that row ends make to Y.
+template <int G, int W, typename VT>
 __global__ void __launch_bounds__(256) stream_spmm(size_t nslots, size_t nslots_pad, size_t seg_slots, size_t nseg,
                                                    const VT *__restrict__ val, const UIN *__restrict__ col,
                                                    const UIN *__restrict__ heads, const UIN *__restrict__ segh,
                                                    const FPT *__restrict__ X, Out o, unsigned il_spl) {
-  constexpr int NG = 32 / G;  // groups per warp = parts per segment
-  const unsigned lane = threadIdx.x & 31u, grp = lane / G, j = lane % G;
+  static_assert(W == 1 || W == 2, "one or two right-hand sides per lane");
+  constexpr int NG = 32 / G;            // groups per warp = parts per segment
+  constexpr int CB = G * W;             // columns of one pass
+  constexpr int SUB = G < 8 ? G : 8;    // slots whose X rows are loaded together
+  const unsigned lane = threadIdx.x & 31u, grp = lane / G, jl = lane % G;
   const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (grp * G));
   const size_t segid = ((size_t)blockIdx.x * 256 + threadIdx.x) >> 5;
   if (segid >= nseg) return;
@@ -48,57 +59,99 @@ __global__ void __launch_bounds__(256) stream_spmm(size_t nslots, size_t nslots_
   for (size_t w = s0 >> 5; w < (a >> 5); w++) cr += __popc(__ldg(heads + w));
   const bool a_head = (__ldg(heads + (a >> 5)) & 1u) != 0;  // a is 32-aligned
   const UIN row_a = a_head ? NO_ROW : cr - 1u;
-  UIN row = cr - 1u;  // current run's row (advanced at each start)
+  UIN row = cr - 1u;    // current run's row (advanced at each start)
   bool have = !a_head;  // the current run has slots in this part
-  double acc = 0.0;
-  const bool live_col = j < o.kb;
+  const unsigned j = jl * W;  // my first column in the block
+  const int ncol = j < o.kb ? min(W, (int)(o.kb - j)) : 0;  // my live columns (0..W)
+  // W-wide loads and stores need 16-byte rows: k even, j0 even, X and Y aligned
+  const bool vec = W == 2 && ncol == 2 && ((o.k | o.j0) & 1u) == 0 &&
+                   ((reinterpret_cast<uintptr_t>(X) | reinterpret_cast<uintptr_t>(o.Y)) & 15u) == 0;
   const size_t xoff = o.j0 + j;
-  if (j == 0) {
+  double acc[W];
+#pragma unroll
+  for (int w = 0; w < W; w++) acc[w] = 0.0;
+  if (jl == 0) {
     o.rec_row[2 * pid] = NO_ROW;
     o.rec_row[2 * pid + 1] = NO_ROW;
   }
-  if (live_col) {
-    o.rec_sum[(2 * pid) * G + j] = 0.0;
-    o.rec_sum[(2 * pid + 1) * G + j] = 0.0;
+#pragma unroll
+  for (int w = 0; w < W; w++) {
+    if (w < ncol) {
+      o.rec_sum[(2 * pid) * CB + j + w] = 0.0;
+      o.rec_sum[(2 * pid + 1) * CB + j + w] = 0.0;
+    }
   }
+  auto put = [&](UIN r) {  // the run of row r ends: Y or the part's head record
+#pragma unroll
+    for (int w = 0; w < W; w++) {
+      if (w < ncol) {
+        if (r == row_a) o.rec_sum[(2 * pid) * CB + j + w] = acc[w];
+        else o.Y[(size_t)real_row(o, r) * o.k + xoff + w] = acc[w];
+      }
+    }
+  };
   for (size_t c0 = a; c0 < b; c0 += G) {
     // one slot per lane of the group, broadcast below
-    const size_t my = c0 + j;
+    const size_t my = c0 + jl;
     const VT mv = val[il_spl ? wide::il_pos(my, il_spl, 16u / sizeof(VT)) : my];
     const UIN mc = col[il_spl ? wide::il_pos(my, il_spl, 4u) : my];
     const UIN hw = __ldg(heads + (c0 >> 5));
-#pragma unroll 4
-    for (int i = 0; i < G; i++) {
-      const size_t s = c0 + i;
-      const VT v = __shfl_sync(gmask, mv, grp * G + i);
-      const UIN c = __shfl_sync(gmask, mc, grp * G + i);
-      if ((hw >> ((s & 31u))) & 1u) {  // a row starts at s: the current run ends
-        if (have && live_col) {
-          if (row == row_a) o.rec_sum[(2 * pid) * G + j] = acc;
-          else {
-            const UIN rr = real_row(o, row);
-            o.Y[(size_t)rr * o.k + xoff] = acc;
-          }
+#pragma unroll
+    for (int i0 = 0; i0 < G; i0 += SUB) {
+      double xv[SUB][W];
+      double vv[SUB];
+#pragma unroll
+      for (int u = 0; u < SUB; u++) {
+        const int i = i0 + u;
+        vv[u] = (double)__shfl_sync(gmask, mv, grp * G + i);
+        const UIN c = __shfl_sync(gmask, mc, grp * G + i);
+        const bool live = c0 + i < nslots;
+        const FPT *xr = X + (size_t)c * o.k + xoff;
+        if (vec) {
+          const double2 q = live ? __ldg(reinterpret_cast<const double2 *>(xr)) : make_double2(0.0, 0.0);
+          xv[u][0] = q.x;
+          xv[u][W - 1] = q.y;
+        } else {
+#pragma unroll
+          for (int w = 0; w < W; w++) xv[u][w] = (live && w < ncol) ? __ldg(xr + w) : 0.0;
         }
-        if (have && row == row_a && j == 0) o.rec_row[2 * pid] = row;
-        row++;
-        acc = 0.0;
-        have = true;
       }
-      if (live_col && s < nslots) acc = fma((double)v, __ldg(X + (size_t)c * o.k + xoff), acc);
+#pragma unroll
+      for (int u = 0; u < SUB; u++) {
+        const size_t s = c0 + i0 + u;
+        if ((hw >> (s & 31u)) & 1u) {  // a row starts at s: the current run ends
+          if (have) {
+            if (vec && row != row_a) {
+              *reinterpret_cast<double2 *>(o.Y + (size_t)real_row(o, row) * o.k + xoff) =
+                  make_double2(acc[0], acc[W - 1]);
+            } else {
+              put(row);
+            }
+            if (row == row_a && jl == 0) o.rec_row[2 * pid] = row;
+          }
+          row++;
+#pragma unroll
+          for (int w = 0; w < W; w++) acc[w] = 0.0;
+          have = true;
+        }
+#pragma unroll
+        for (int w = 0; w < W; w++) acc[w] = fma(vv[u], xv[u][w], acc[w]);
+      }
     }
   }
   // the run open at the part's end
   if (have) {
     const bool is_a = row == row_a;
-    if (j == 0) o.rec_row[2 * pid + (is_a ? 0 : 1)] = row;
-    if (live_col) o.rec_sum[(2 * pid + (is_a ? 0 : 1)) * G + j] = acc;
+    if (jl == 0) o.rec_row[2 * pid + (is_a ? 0 : 1)] = row;
+#pragma unroll
+    for (int w = 0; w < W; w++)
+      if (w < ncol) o.rec_sum[(2 * pid + (is_a ? 0 : 1)) * CB + j + w] = acc[w];
   }
 }
 
 // Record i (of 2 per part) writes its row if it is that row's last record,
 // adding the row's earlier records; rows with no slot get zeros.
-template <int G>
+template <int G>  // G = columns of one pass
 __global__ void spmm_fixup(size_t nrec, const UIN *__restrict__ rec_row, const double *__restrict__ rec_sum,
                            const UIN *__restrict__ empty, size_t nempty, Out o) {
   const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;

@@ -19,7 +19,8 @@ COMBOS = [("CSR", "rows"), ("CSR", "ldg"), ("CSR", "tma"), ("AXC", "rows"), ("AX
           ("K1", "auto"), ("K1P", "auto"), ("NOC1", "ldg"), ("NOC1", "tma"), ("NOC4", "ldg"), ("NOC4", "tma"),
           ("NOC8", "ldg"), ("NOC8", "tma"), ("NOC16", "ldg"), ("NOC16", "tma"), ("NOC3", "ldg"),
           ("COM128", "ldg"), ("COM128", "tma"), ("COM256", "ldg"), ("COM512", "tma"),
-          ("COM128", "wide"), ("NOC1", "wide"), ("AXC", "wide"), ("CSR", "wide")]
+          ("COM128", "wide"), ("NOC1", "wide"), ("AXC", "wide"), ("CSR", "wide"), ("NOC4", "wide"), ("NOC8", "wide"),
+          ("NOC3", "wide"), ("NOC16", "auto"), ("CSR", "auto"), ("AXC", "auto")]
 KIDS = {"ldg": 1, "tma": 2, "rows": 3, "wide": 4}
 WIDE_VARIANTS = list(range(35))
 
@@ -284,12 +285,13 @@ def powerlaw4m(env):
 @pytest.mark.parametrize("fmt,kernel", [("CSR", "rows"), ("CSR", "ldg"), ("AXC", "rows"), ("AXC", "ldg"),
                                         ("K1P", "auto"), ("NOC1", "ldg"), ("NOC1", "tma"), ("NOC4", "ldg"),
                                         ("NOC4", "tma"), ("NOC8", "tma"), ("COM128", "ldg"), ("COM128", "tma"),
-                                        ("COM512", "ldg"), ("COM128", "wide"), ("NOC1", "wide"), ("CSR", "wide")])
+                                        ("COM512", "ldg"), ("COM128", "wide"), ("NOC1", "wide"), ("CSR", "wide"),
+                                        ("NOC4", "auto"), ("NOC8", "auto"), ("AXC", "auto"), ("K1", "auto")])
 def test_powerlaw_4m(env, powerlaw4m, fmt, kernel):
     row, col, val, x = powerlaw4m
     p, _ = check_plan(env, row, col, val, x, fmt, kernel=kernel)
     assert p.status() == 0
-    if (fmt, kernel) in (("COM128", "ldg"), ("NOC1", "ldg"), ("COM128", "wide")):
+    if (fmt, kernel) in (("COM128", "ldg"), ("NOC1", "ldg"), ("COM128", "wide"), ("NOC4", "auto"), ("K1", "auto")):
         check_plan(env, row, col, val, x, fmt, val_kind="f32", kernel=kernel)
 
 
