@@ -374,8 +374,9 @@ def main(argv=None):
     if not a.no_formats:
         variants = [(f, "f64", "u32", "auto") for f in ["CSR", "AXC", "K1", "K1P", "NOC1", "NOC4", "NOC8",
                                                            "NOC16", "COM128", "COM256", "COM512"]]
-        variants += [("CSR", "f64", "u32", "wide"), ("AXC", "f64", "u32", "wide"), ("NOC1", "f64", "u32", "ldg"),
-                     ("COM128", "f64", "u32", "ldg"), ("NOC4", "f64", "u32", "tma"), ("COM128", "f64", "u32", "tma")]
+        variants += [("CSR", "f64", "u32", "rows"), ("AXC", "f64", "u32", "rows"), ("NOC1", "f64", "u32", "ldg"),
+                     ("COM128", "f64", "u32", "ldg"), ("NOC4", "f64", "u32", "ldg"), ("NOC8", "f64", "u32", "ldg"),
+                     ("NOC4", "f64", "u32", "tma"), ("COM128", "f64", "u32", "tma")]
         variants += [(f, vk, ck, "auto") for f in ("COM128", "NOC1")
                      for vk, ck in (("f32", "u32"), ("f64", "d16"), ("f32", "d16"))]
         variants += [(f, vk, ck, "ldg") for f in ("COM128", "NOC1")
