@@ -280,6 +280,8 @@ def main(argv=None):
     ap.add_argument("--batch-nmax", type=float, default=2e5, help="largest n of the batched matrices")
     ap.add_argument("--no-formats", action="store_true", help="skip the per-format table")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the SpMM and batched lines (1M-row SpMM k = 8/16/32; 512 banded matrices)")
     ap.add_argument("--no-precision", action="store_true",
                     help="skip the FP64 / FP32-value lines on the 27-point stencil 160^3")
     ap.add_argument("--cpu-budget", type=float, default=15.0, help="seconds of reference CPU work")
@@ -446,6 +448,19 @@ def main(argv=None):
         except Exception as e:  # the extra lines must not sink the headline
             precision = {"unavailable": str(e)[:160]}
 
+    # multi-RHS SpMM (AUTO's plan) and the 512 batched matrices in one graph
+    # launch, on one GPU (rank 0 of a single-process run)
+    spmm = batched = None
+    if ws == 1 and not a.no_extras:
+        try:
+            spmm, _ = spmm_lines(max(20, min(a.steps, 200)), 5, False, peak)
+        except Exception as e:  # the extra lines must not sink the headline
+            spmm = {"unavailable": str(e)[:160]}
+        try:
+            batched = batch_lines(a, max(20, min(a.steps, 200)), 5, peak)
+        except Exception as e:
+            batched = {"unavailable": str(e)[:160]}
+
     # format conversion: the host builder (OpenMP, the reference's layout
     # rules) against the same conversion on the GPU, for the compacted AXT
     conversion = None
@@ -521,6 +536,8 @@ def main(argv=None):
             "parity": check,
             "formats": formats,
             "precision": precision,
+            "spmm": spmm,
+            "batched": batched,
             "conversion": conversion,
         }
         print(json.dumps(out), flush=True)
@@ -600,50 +617,66 @@ def _event_time(fn, steps: int, warmup: int) -> float:
     return e0.elapsed_time(e1) / 1e3 / steps
 
 
-def main_spmm(a, rank, ws, W):
+def spmm_lines(steps: int, warmup: int, tuned: bool, peak: float):
     """Y = A X on the power-law generator at n = 1,000,000 (seed 3), X n x k
-    row-major U[-1, 1], k in {8, 16, 32}, FP64 and FP32 values; the plan
-    (format, kernel, RHS block) is the autotuner's choice for the matrix."""
+    row-major U[-1, 1], k in {8, 16, 32}, FP64 and FP32 values.  The plan is
+    the autotuner's choice (tuned) or AUTO's compacted AXT (bs 128).  Per
+    (value form, k): time, GFLOP/s, GB/s and the HBM fraction of
+    nnz*(b_val + 4) + n*k*16 + 4*(n+1) (A read once, X and Y once), and the
+    error of every column against the oracle.  Returns (results, launches)."""
     import torch
-    torch.cuda.set_device(0)
     from int_spmv_b200 import _lib, autotune
+    from int_spmv_b200 import device as D
     from int_spmv_b200 import formats as F
     from oracle import Oracle
     wl = make_workload("powerlaw1m")
     csr = F.CSR(wl["row"], wl["col"], wl["val"])
     n, nnz = csr.n, csr.nnz
     orc = Oracle()
-    peak, peak_src = hbm_peak()
+    com = None if tuned else F.getFormatDataAXT(0, 128, 8, 1, "COM", csr, wl["x"])[1]
     res, launches = {}, 0
     for val in ("f64", "f32"):
         for k in (8, 16, 32):
-            plan, choice = autotune.best_plan(csr, wl["x"], val=val, k=k, use_cache=False)
+            if tuned:
+                plan, choice = autotune.best_plan(csr, wl["x"], val=val, k=k, use_cache=False)
+            else:
+                plan, choice = D.Plan(csr, com, val=val), {"format": "COM128", "kwargs": {}}
             X = torch.from_numpy(np.random.default_rng(3).uniform(-1, 1, (n, k))).cuda()
             Y = torch.empty_like(X)
             l0 = _lib.launch_count()
             plan.spmm(X, Y)
             per = _lib.launch_count() - l0
-            t = _event_time(lambda: plan.spmm(X, Y), a.steps, W)
-            launches += per * a.steps
+            t = _event_time(lambda: plan.spmm(X, Y), steps, warmup)
+            launches += per * steps
+            plan.spmm(X, Y)
             Yh, Xh = Y.cpu().numpy(), X.cpu().numpy()
             err = 0.0
-            for j in (0, k // 2, k - 1):
+            for j in range(k):
                 xj = np.ascontiguousarray(Xh[:, j])
                 ref, ab = orc.cf_csr(wl["row"], wl["col"], wl["val"], xj), orc.abs_csr(wl["row"], wl["col"], wl["val"], xj)
                 err = max(err, float(np.max(np.abs(Yh[:, j] - ref) / np.maximum(ab, 1e-300))))
             bval = 8 if val == "f64" else 4
-            # nnz*(b_val + b_idx) + n*k*(b_x + b_y) + 4*(n+1): A read once, X and Y once
             B = nnz * (bval + 4) + n * k * 16 + 4 * (n + 1)
             res[f"{val}/k{k}"] = {"ms": t * 1e3, "gflops": 2 * nnz * k / t / 1e9, "gbs": B / t / 1e9,
                                   "alg_bytes": B, "frac": B / t / 1e9 / peak, "kernel": plan.kernel_name(),
                                   "format": choice["format"], "kwargs": choice["kwargs"],
-                                  "max_componentwise_err": err, "rhs_columns_checked": 3}
-            del plan
+                                  "max_componentwise_err": err, "bound": 1e-12 if val == "f64" else 1e-6,
+                                  "rhs_columns_checked": k}
+            del plan, X, Y
+    return dict(workload="spmm_powerlaw_n1M_seed3", n=n, nnz=nnz, steps=steps, **res), launches
+
+
+def main_spmm(a, rank, ws, W):
+    """The SpMM workload alone (spmm_lines with the autotuner's plans)."""
+    import torch
+    torch.cuda.set_device(0)
+    peak, peak_src = hbm_peak()
+    res, launches = spmm_lines(a.steps, W, True, peak)
     best = res["f64/k32"]
     out = {"metric": "SpMM GFLOP/s (2*nnz*k)", "value": best["gflops"], "unit": "GFLOP/s", "n_gpus": 1,
            "steps": a.steps, "warmup": W, "ms_per_step": best["ms"], "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "data": "synthetic: power-law n=1,000,000 seed 3, X~U[-1,1]",
-           "config": {"workload": "spmm_powerlaw_n1M_seed3", "n": n, "nnz": nnz, "k": [8, 16, 32],
+           "config": {"workload": "spmm_powerlaw_n1M_seed3", "n": res["n"], "nnz": res["nnz"], "k": [8, 16, 32],
                       "choice": "autotuned per (value form, k)"},
            "gpu_launches": launches,
            "roofline": {"bound": "hbm", "achieved": best["gbs"], "peak": peak, "unit": "GB/s",
@@ -653,14 +686,14 @@ def main_spmm(a, rank, ws, W):
     print(json.dumps(out), flush=True)
 
 
-def main_batch(a, rank, ws, W):
+def batch_lines(a, steps: int, warmup: int, peak: float) -> dict:
     """Many uneven FEM-like banded matrices (n log-uniform in [1e3, nmax],
     rows of 7-81 entries within +/-3*rl of the diagonal; seed 4), each with
     its own x: one block-diagonal plan in one CUDA-graph launch (the
     lane-interleaved kernel, and the persistent work-queue kernel), against
-    one plan per matrix launched one after the other."""
+    one plan per matrix launched one after the other.  Every matrix of the
+    graph launch is checked against its own oracle product."""
     import torch
-    torch.cuda.set_device(0)
     from int_spmv_b200 import _lib
     from int_spmv_b200 import batch as BT
     from int_spmv_b200 import device as D
@@ -681,10 +714,13 @@ def main_batch(a, rank, ws, W):
         plan.spmv_graph(xt, y)  # captures the product's kernels, then launches the graph once
         in_graph = _lib.launch_count() - l0 - 1
         torch.cuda.synchronize()
-        t = _event_time(lambda: plan.spmv_graph(xt, y), a.steps, W)
-        res[name] = {"ms": t * 1e3, "gflops": 2 * nnz / t / 1e9, "gbs": plan.info["alg_bytes"] / t / 1e9,
+        t = _event_time(lambda: plan.spmv_graph(xt, y), steps, warmup)
+        bb = plan.info["alg_bytes"]
+        res[name] = {"ms": t * 1e3, "gflops": 2 * nnz / t / 1e9, "gbs": bb / t / 1e9, "frac": bb / t / 1e9 / peak,
                      "kernel": plan.kernel_name(), "graph_launches_per_step": 1, "kernels_in_graph": in_graph}
-        yb = y.cpu().numpy()
+        if name == "graph_wide":
+            plan.spmv_graph(xt, y)
+            yb = y.cpu().numpy()
         del plan
     del big
     # one plan per matrix, launched one after the other (2 launches each)
@@ -701,30 +737,40 @@ def main_batch(a, rank, ws, W):
     l0 = _lib.launch_count()
     each()
     per = _lib.launch_count() - l0
-    t = _event_time(each, max(3, a.steps // 4), W)
+    t = _event_time(each, max(3, steps // 4), warmup)
     res["separate"] = {"ms": t * 1e3, "gflops": 2 * nnz / t / 1e9, "launches_per_step": per}
-    ys_sep = y.cpu().numpy()
-    # parity: every matrix of a sample against the oracle, and the batched y
+    del plans
+    # parity: every matrix of the graph launch against the oracle
     orc, err = Oracle(), 0.0
     tol = 1e-12 if a.val == "f64" else 1e-6
-    for m in sorted(set(np.linspace(0, len(mats) - 1, 16).astype(int))):
-        row, col, val = mats[m]
+    for m, (row, col, val) in enumerate(mats):
         a0, a1 = int(off[m]), int(off[m + 1])
         ref, ab = orc.cf_csr(row, col, val, x[a0:a1]), orc.abs_csr(row, col, val, x[a0:a1])
-        for yy in (yb, ys_sep):
-            err = max(err, float(np.max(np.abs(yy[a0:a1] - ref) / np.maximum(ab, 1e-300))))
-    out = {"metric": "batched SpMV GFLOP/s (2*sum nnz)", "value": res["graph_wide"]["gflops"], "unit": "GFLOP/s",
-           "n_gpus": 1, "steps": a.steps, "warmup": W, "ms_per_step": res["graph_wide"]["ms"],
+        err = max(err, float(np.max(np.abs(yb[a0:a1] - ref) / np.maximum(ab, 1e-300))))
+    return {"workload": f"fem_batch_{a.batch_count}_nmax{a.batch_nmax:g}", "matrices": len(mats), "n": n, "nnz": nnz,
+            "value_kind": a.val, "steps": steps, "results": res,
+            "speedup_graph_vs_separate": res["separate"]["ms"] / res["graph_wide"]["ms"],
+            "parity": {"max_componentwise": err, "bound": tol, "pass": err <= tol, "matrices_checked": len(mats)},
+            "setup_s": time.time() - t0}
+
+
+def main_batch(a, rank, ws, W):
+    """The batched workload alone (batch_lines)."""
+    import torch
+    torch.cuda.set_device(0)
+    peak, _ = hbm_peak()
+    r = batch_lines(a, a.steps, W, peak)
+    g = r["results"]["graph_wide"]
+    out = {"metric": "batched SpMV GFLOP/s (2*sum nnz)", "value": g["gflops"], "unit": "GFLOP/s",
+           "n_gpus": 1, "steps": a.steps, "warmup": W, "ms_per_step": g["ms"],
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
            "dtype": "f64" if a.val == "f64" else "f32-mul/f64-acc",
            "data": f"synthetic: {a.batch_count} banded FEM-like matrices, n log-uniform in [1e3, {a.batch_nmax:g}], "
                    "rl U[7,81] within +/-3 rl, seed 4 (int_spmv_b200/matrices.py fem_batch_c)",
-           "config": {"workload": f"fem_batch_{a.batch_count}_nmax{a.batch_nmax:g}", "matrices": len(mats),
-                      "n": n, "nnz": nnz, "value_kind": a.val},
-           "speedup_graph_vs_separate": res["separate"]["ms"] / res["graph_wide"]["ms"],
-           "gpu_launches": a.steps * res["graph_wide"]["kernels_in_graph"],
-           "parity": {"max_componentwise": err, "bound": tol, "pass": err <= tol, "matrices_checked": 16},
-           "results": res, "setup_s": time.time() - t0}
+           "config": {"workload": r["workload"], "matrices": r["matrices"], "n": r["n"], "nnz": r["nnz"],
+                      "value_kind": a.val},
+           "gpu_launches": a.steps * g["kernels_in_graph"], **{k: r[k] for k in ("speedup_graph_vs_separate",
+                                                                                 "parity", "results", "setup_s")}}
     print(json.dumps(out), flush=True)
 
 
