@@ -79,6 +79,7 @@ struct ispmv_plan_s {
   double *mm_sum = nullptr;
   size_t mm_cap = 0;                 // doubles in mm_sum
   size_t mm_rows_cap = 0;            // entries of mm_row
+  UIN k1_long = 0;                   // K1: leading chunks run a warp each
   std::vector<void *> owned;
   ispmv_plan_info info{};
   std::vector<cudaEvent_t> tev;      // kernel timing: event pairs around the main kernel (a ring)
@@ -92,6 +93,7 @@ namespace {
 
 constexpr size_t SS = sss::SS;      // slots per staged stage; streams pad to it
 constexpr size_t SEG_SLOTS = 2048;  // default slots per warp segment
+constexpr UIN K1_LONG = 64;         // K1 chunks of at least this many columns run a warp each
 
 #define TRY(expr)        \
   do {                   \
@@ -1148,6 +1150,10 @@ ISPMV_API int ispmv_plan_k1(const str_matCSR *csr, const str_matK1 *k1, int reor
   p->nnz = csr->nnz;
   p->slots = k1->lenVC;
   p->chunkNum = k1->chunkNum;
+  // the long chunks (a warp each): the prefix of chunks with at least
+  // K1_LONG columns (nmc never increases: rows are sorted by length)
+  p->k1_long = 0;
+  while (p->k1_long < k1->chunkNum && k1->nmc[p->k1_long] >= K1_LONG) p->k1_long++;
   std::vector<double> v(k1->val, k1->val + k1->lenVC);
   int st = upload_values(p, v);
   if (!st) st = dev_upload(p, k1->col, k1->lenVC, &p->col);
@@ -1705,14 +1711,14 @@ int run_main(ispmv_plan_s *p, const FPT *x, FPT *y, int beta, cudaStream_t s) {
       return check_launch("csr_vec");
     }
     case P_K1: {
-      const unsigned g = (unsigned)(((size_t)p->chunkNum * 8 + pk::TPB - 1) / pk::TPB);
+      const unsigned g = (unsigned)((pk::k1_warps(p->chunkNum, p->k1_long) * 32 + pk::TPB - 1) / pk::TPB);
       if (p->fmt == F_K1P) {
-        pk::k1_chunks<VT, true><<<g, pk::TPB, 0, s>>>(p->n, p->chunkNum, p->chp, p->nmc, p->permi, p->col, val, x, y,
-                                                      beta);
+        pk::k1_chunks<VT, true><<<g, pk::TPB, 0, s>>>(p->n, p->chunkNum, p->k1_long, p->chp, p->nmc, p->permi,
+                                                      p->col, val, x, y, beta);
         return check_launch("k1_chunks<scatter>");
       }
-      pk::k1_chunks<VT, false><<<g, pk::TPB, 0, s>>>(p->n, p->chunkNum, p->chp, p->nmc, p->permi, p->col, val, x,
-                                                     p->res, beta);
+      pk::k1_chunks<VT, false><<<g, pk::TPB, 0, s>>>(p->n, p->chunkNum, p->k1_long, p->chp, p->nmc, p->permi,
+                                                     p->col, val, x, p->res, beta);
       return check_launch("k1_chunks");
     }
     case P_STREAM:
@@ -1743,6 +1749,11 @@ ISPMV_API int ispmv_plan_spmv_graph(ispmv_plan p, const FPT *x, FPT *y, int beta
     p->graph_exec = nullptr;
     p->graph = nullptr;
     if (!p->cap_stream) ISPMV_TRY(cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking));
+    // work areas a product allocates on first use, allocated before the
+    // capture (no allocation may happen inside it): the FP32 copy of x of
+    // FP32-value plans on the lane-interleaved kernel
+    if (p->opts.val_kind != ISPMV_VAL_F64 && p->opts.kernel == ISPMV_KERNEL_WIDE && !p->x32)
+      TRY(dev_alloc(p, p->n, &p->x32));
     ISPMV_TRY(cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal));
     p->capturing = true;
     const int st = p->opts.val_kind == ISPMV_VAL_F64 ? run<double>(p, x, y, beta, p->cap_stream)
@@ -1750,11 +1761,13 @@ ISPMV_API int ispmv_plan_spmv_graph(ispmv_plan p, const FPT *x, FPT *y, int beta
     p->capturing = false;
     cudaGraph_t g = nullptr;
     const cudaError_t e = cudaStreamEndCapture(p->cap_stream, &g);
-    if (st) {
+    if (st || e != cudaSuccess) {
       if (g) cudaGraphDestroy(g);
-      return st;
+      // a failed capture leaves its error as the runtime's last error: clear
+      // it so that it is not reported again by a later, unrelated call
+      (void)cudaGetLastError();
+      return st ? st : cuda_status(e, "cudaStreamEndCapture");
     }
-    if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture");
     p->graph = g;
     ISPMV_TRY(cudaGraphInstantiate(&p->graph_exec, p->graph, 0));
     p->g_x = x;

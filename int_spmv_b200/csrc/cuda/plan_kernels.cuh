@@ -70,36 +70,33 @@ __global__ void __launch_bounds__(TPB) axc_rows(UIN n, const UIN *__restrict__ b
 }
 
 // ----------------------------------------------------------------- K1 --
-// 8 lanes per chunk (lane = row of the chunk: each chunk column is one
-// coalesced 64-byte load); SCATTER writes y[permi] (K1 with integrated
-// reordering), else res in chunk order (then k1_order).  K1 orders rows by
-// length, so a chunk's rows are unrelated rows of the matrix and nearly
-// every gather misses the lines its neighbours touched: the column loop is
-// unrolled U = 8 deep with independent sums, so a lane's 8 value/column
-// loads and then its 8 gathers are in flight together.
-template <typename VT, bool SCATTER>
-__global__ void __launch_bounds__(TPB) k1_chunks(UIN n, UIN chunkNum, const UIN *__restrict__ chp,
-                                                 const UIN *__restrict__ nmc, const UIN *__restrict__ permi,
-                                                 const UIN *__restrict__ col, const VT *__restrict__ val,
-                                                 const FPT *__restrict__ x, FPT *__restrict__ out, int beta) {
+// K1 orders rows by length (descending), so a chunk's rows are unrelated
+// rows of the matrix and nearly every gather misses the lines its
+// neighbours touched; the chunks' column counts nmc never increase.  The
+// first `nlong` chunks (the long ones) get a warp each: 4 groups of 8 lanes
+// (lane = row of the chunk) take every 4th column, 8 columns at a time, and
+// combine their sums with two shuffles.  The rest go 4 chunks to a warp,
+// 8 lanes each, also 8 columns at a time.  A lane keeps its 8 value/column
+// loads and then its 8 gathers in flight together, with independent sums.
+// SCATTER writes y[permi] (K1 with integrated reordering), else res in
+// chunk order (then k1_order).  Every chunk column is one coalesced 64-byte
+// load of values.
+template <typename VT, int STRIDE>
+__device__ __forceinline__ double k1_sum(const VT *__restrict__ val, const UIN *__restrict__ col,
+                                         const FPT *__restrict__ x, size_t off, UIN k0, UIN m, unsigned lane8) {
   constexpr int U = 8;
-  const unsigned lane8 = threadIdx.x & 7u;
-  const size_t c = ((size_t)blockIdx.x * TPB + threadIdx.x) >> 3;
-  if (c >= chunkNum) return;
-  const size_t off = chp[c];
-  const UIN m = nmc[c];
   double acc[U];
 #pragma unroll
   for (int u = 0; u < U; u++) acc[u] = 0.0;
-  UIN k = 0;
-  for (; k + U <= m; k += U) {
+  UIN k = k0;
+  for (; k + (U - 1) * STRIDE < m; k += U * STRIDE) {
     const size_t p = off + (size_t)k * 8 + lane8;
     VT v[U];
     UIN cc[U];
 #pragma unroll
     for (int u = 0; u < U; u++) {
-      v[u] = ld_stream(val + p + 8 * u);
-      cc[u] = ld_stream(col + p + 8 * u);
+      v[u] = ld_stream(val + p + (size_t)8 * STRIDE * u);
+      cc[u] = ld_stream(col + p + (size_t)8 * STRIDE * u);
     }
     double xv[U];
 #pragma unroll
@@ -108,13 +105,36 @@ __global__ void __launch_bounds__(TPB) k1_chunks(UIN n, UIN chunkNum, const UIN 
     for (int u = 0; u < U; u++) acc[u] = fmac<VT>(v[u], xv[u], acc[u]);
   }
 #pragma unroll
-  for (int u = 0; u < U; u++) {  // the chunk's last m % U columns
-    if (k + u < m) {
-      const size_t p = off + (size_t)(k + u) * 8 + lane8;
+  for (int u = 0; u < U; u++) {  // the last columns of this lane's share
+    const UIN kk = k + (UIN)(u * STRIDE);
+    if (kk < m) {
+      const size_t p = off + (size_t)kk * 8 + lane8;
       acc[u] = fmac<VT>(ld_stream(val + p), ldg(x + ld_stream(col + p)), acc[u]);
     }
   }
-  const double s = ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+  return ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+}
+
+template <typename VT, bool SCATTER>
+__global__ void __launch_bounds__(TPB) k1_chunks(UIN n, UIN chunkNum, UIN nlong, const UIN *__restrict__ chp,
+                                                 const UIN *__restrict__ nmc, const UIN *__restrict__ permi,
+                                                 const UIN *__restrict__ col, const VT *__restrict__ val,
+                                                 const FPT *__restrict__ x, FPT *__restrict__ out, int beta) {
+  const unsigned lane = threadIdx.x & 31u, lane8 = lane & 7u;
+  const size_t w = ((size_t)blockIdx.x * TPB + threadIdx.x) >> 5;
+  size_t c;
+  double s;
+  if (w < nlong) {  // one warp per long chunk: group g takes columns g, g + 4, ...
+    c = w;
+    s = k1_sum<VT, 4>(val, col, x, chp[c], lane >> 3, nmc[c], lane8);
+    s += __shfl_xor_sync(FULL, s, 8);
+    s += __shfl_xor_sync(FULL, s, 16);
+    if (lane >= 8) return;
+  } else {
+    c = nlong + (w - nlong) * 4 + (lane >> 3);
+    if (c >= chunkNum) return;
+    s = k1_sum<VT, 1>(val, col, x, chp[c], 0, nmc[c], lane8);
+  }
   const size_t i = c * 8 + lane8;
   if (SCATTER) {
     if (i < n) {
@@ -125,6 +145,9 @@ __global__ void __launch_bounds__(TPB) k1_chunks(UIN n, UIN chunkNum, const UIN 
     out[i] = s;
   }
 }
+
+// Warps of a K1 launch: one per long chunk, one per 4 other chunks.
+inline size_t k1_warps(UIN chunkNum, UIN nlong) { return (size_t)nlong + ((size_t)(chunkNum - nlong) + 3) / 4; }
 
 __global__ void k1_order(UIN n, const UIN *__restrict__ permi, const FPT *__restrict__ res, FPT *__restrict__ y,
                          int beta) {

@@ -30,12 +30,15 @@ struct Out {
 __device__ __forceinline__ UIN real_row(const Out &o, UIN r) { return o.rowmap ? o.rowmap[r] : r; }
 
 // G lanes per group, W (1 or 2) consecutive right-hand sides per lane: a
-// pass covers CB = G*W columns.  Per step the group loads G slots (one per
-// lane) and then works through them SUB at a time in two phases: first the
-// X rows of all SUB slots are loaded into registers (W-wide vector loads of
-// the group's contiguous piece of each row), then the row starts are
-// handled and the products accumulated.  The loads of a sub-batch are thus
-// in flight together, ahead of the stores that row ends make to Y.
+// pass covers CB = G*W columns.  A step of the group covers T = G*R slots
+// (R = 8/G slots per lane for G < 8, else 1): each lane loads R slots'
+// values and columns (coalesced), one step ahead of their use, and the
+// group then works through the step's slots 8 at a time in two phases:
+// first the X rows of all 8 slots are loaded into registers (W-wide vector
+// loads of the group's contiguous piece of each row), then the row starts
+// are handled and the products accumulated.  The loads of a step are thus in
+// flight together, ahead of the stores that row ends make to Y, and the
+// values and columns of the next step arrive meanwhile.
 template <int G, int W, typename VT>
 __global__ void __launch_bounds__(256) stream_spmm(size_t nslots, size_t nslots_pad, size_t seg_slots, size_t nseg,
                                                    const VT *__restrict__ val, const UIN *__restrict__ col,
@@ -44,7 +47,9 @@ __global__ void __launch_bounds__(256) stream_spmm(size_t nslots, size_t nslots_
   static_assert(W == 1 || W == 2, "one or two right-hand sides per lane");
   constexpr int NG = 32 / G;            // groups per warp = parts per segment
   constexpr int CB = G * W;             // columns of one pass
-  constexpr int SUB = G < 8 ? G : 8;    // slots whose X rows are loaded together
+  constexpr int R = G < 8 ? 8 / G : 1;  // slots per lane and step
+  constexpr int T = G * R;              // slots per step (8, 16 or 32: within one bitmap word)
+  constexpr int SUB = 8;                // slots whose X rows are loaded together
   const unsigned lane = threadIdx.x & 31u, grp = lane / G, jl = lane % G;
   const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (grp * G));
   const size_t segid = ((size_t)blockIdx.x * 256 + threadIdx.x) >> 5;
@@ -90,27 +95,44 @@ __global__ void __launch_bounds__(256) stream_spmm(size_t nslots, size_t nslots_
       }
     }
   };
-  for (size_t c0 = a; c0 < b; c0 += G) {
-    // one slot per lane of the group, broadcast below
-    const size_t my = c0 + jl;
-    const VT mv = val[il_spl ? wide::il_pos(my, il_spl, 16u / sizeof(VT)) : my];
-    const UIN mc = col[il_spl ? wide::il_pos(my, il_spl, 4u) : my];
-    const UIN hw = __ldg(heads + (c0 >> 5));
+  // the step's slots: lane jl holds slots c0 + q*G + jl, q < R
+  VT nv[R];
+  UIN nc[R], nhw = 0;
+  auto load_step = [&](size_t c0) {
 #pragma unroll
-    for (int i0 = 0; i0 < G; i0 += SUB) {
+    for (int q = 0; q < R; q++) {
+      const size_t my = c0 + (size_t)q * G + jl;
+      nv[q] = val[il_spl ? wide::il_pos(my, il_spl, 16u / sizeof(VT)) : my];
+      nc[q] = col[il_spl ? wide::il_pos(my, il_spl, 4u) : my];
+    }
+    nhw = __ldg(heads + (c0 >> 5));
+  };
+  if (a < b) load_step(a);
+  for (size_t c0 = a; c0 < b; c0 += T) {
+    VT mv[R];
+    UIN mc[R];
+#pragma unroll
+    for (int q = 0; q < R; q++) {
+      mv[q] = nv[q];
+      mc[q] = nc[q];
+    }
+    const UIN hw = nhw;
+    if (c0 + T < b) load_step(c0 + T);
+#pragma unroll
+    for (int i0 = 0; i0 < T; i0 += SUB) {
       double xv[SUB][W];
       double vv[SUB];
 #pragma unroll
       for (int u = 0; u < SUB; u++) {
-        const int i = i0 + u;
-        vv[u] = (double)__shfl_sync(gmask, mv, grp * G + i);
-        const UIN c = __shfl_sync(gmask, mc, grp * G + i);
+        const int i = i0 + u;  // slot c0 + i: lane i % G, register i / G
+        vv[u] = (double)__shfl_sync(gmask, mv[i / G], grp * G + i % G);
+        const UIN c = __shfl_sync(gmask, mc[i / G], grp * G + i % G);
         const bool live = c0 + i < nslots;
         const FPT *xr = X + (size_t)c * o.k + xoff;
         if (vec) {
-          const double2 q = live ? __ldg(reinterpret_cast<const double2 *>(xr)) : make_double2(0.0, 0.0);
-          xv[u][0] = q.x;
-          xv[u][W - 1] = q.y;
+          const double2 qx = live ? __ldg(reinterpret_cast<const double2 *>(xr)) : make_double2(0.0, 0.0);
+          xv[u][0] = qx.x;
+          xv[u][W - 1] = qx.y;
         } else {
 #pragma unroll
           for (int w = 0; w < W; w++) xv[u][w] = (live && w < ncol) ? __ldg(xr + w) : 0.0;

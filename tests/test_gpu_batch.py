@@ -85,3 +85,30 @@ def test_autotune_picks_and_caches(tmp_path, monkeypatch):
     assert_parity(y, orc.cf_csr(row, col, val, x), orc.abs_csr(row, col, val, x), TOL_F64, what="tuned plan")
     ck = T.tune(csr, x, k=16, reps=3)
     assert ck["kwargs"]["rhs_block"] in (8, 16, 32)
+
+
+@pytest.mark.parametrize("val_kind,kw", [("f32", dict(kernel="wide")), ("f32", dict(kernel="wide", variant=32)),
+                                         ("f64", dict(kernel="wide", variant=26)), ("f64", dict(kernel="ldg", variant=16)),
+                                         ("f32", dict(kernel="ldg", variant=16))])
+def test_graph_capture_as_first_product(val_kind, kw):
+    """A plan whose first product is the graph launch: its per-product work
+    areas (the FP32 copy of x) exist before the capture begins, and the
+    captured graph gives the oracle's product; plain products after it too."""
+    import torch
+
+    from int_spmv_b200 import device as D
+    from int_spmv_b200 import formats as F
+    from int_spmv_b200 import matrices as M
+    from oracle import Oracle
+    row, col, val = M.random_csr(30011, 9, rl_max=40, empty_frac=0.05)
+    x = M.uniform_x(30011, 9)
+    csr = F.CSR(row, col, val)
+    orc = Oracle()
+    ref, ab = orc.cf_csr(row, col, val, x), orc.abs_csr(row, col, val, x)
+    tol = TOL_F64 if val_kind == "f64" else TOL_F32
+    p = D.Plan(csr, F.getFormatDataAXT(0, 128, 8, 1, "COM", csr, x)[1], val=val_kind, **kw)
+    xt = torch.from_numpy(x).cuda()
+    y = torch.full((30011,), 3.0, dtype=torch.float64, device="cuda")
+    p.spmv_graph(xt, y)
+    assert_parity(y.cpu().numpy(), ref, ab, tol, what=f"graph first {val_kind} {kw}")
+    assert_parity(p.spmv(xt).cpu().numpy(), ref, ab, tol, what=f"plain after graph {val_kind} {kw}")
