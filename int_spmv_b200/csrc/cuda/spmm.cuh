@@ -30,10 +30,10 @@ struct Out {
 __device__ __forceinline__ UIN real_row(const Out &o, UIN r) { return o.rowmap ? o.rowmap[r] : r; }
 
 // G lanes per group, W (1 or 2) consecutive right-hand sides per lane: a
-// pass covers CB = G*W columns.  A step of the group covers T = G*R slots
-// (R = 8/G slots per lane for G < 8, else 1): each lane loads R slots'
-// values and columns (coalesced), one step ahead of their use, and the
-// group then works through the step's slots 8 at a time in two phases:
+// pass covers CB = G*W columns.  A step of the group covers T = G slots:
+// each lane loads one slot's value and column (coalesced), one step ahead
+// of their use, and the group then works through the step's slots (8 at a
+// time when G = 16) in two phases:
 // first the X rows of all 8 slots are loaded into registers (W-wide vector
 // loads of the group's contiguous piece of each row), then the row starts
 // are handled and the products accumulated.  The loads of a step are thus in
@@ -47,9 +47,9 @@ __global__ void __launch_bounds__(256) stream_spmm(size_t nslots, size_t nslots_
   static_assert(W == 1 || W == 2, "one or two right-hand sides per lane");
   constexpr int NG = 32 / G;            // groups per warp = parts per segment
   constexpr int CB = G * W;             // columns of one pass
-  constexpr int R = G < 8 ? 8 / G : 1;  // slots per lane and step
-  constexpr int T = G * R;              // slots per step (8, 16 or 32: within one bitmap word)
-  constexpr int SUB = 8;                // slots whose X rows are loaded together
+  constexpr int R = 1;                  // slots per lane and step
+  constexpr int T = G * R;              // slots per step (4, 8 or 16: within one bitmap word)
+  constexpr int SUB = T < 8 ? T : 8;    // slots whose X rows are loaded together
   const unsigned lane = threadIdx.x & 31u, grp = lane / G, jl = lane % G;
   const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << (grp * G));
   const size_t segid = ((size_t)blockIdx.x * 256 + threadIdx.x) >> 5;

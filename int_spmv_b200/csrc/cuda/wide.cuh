@@ -242,8 +242,13 @@ __device__ __forceinline__ void batch(const VT (&v)[SPL], const XT (&xv)[SPL], u
   const int start = F ? 31 - __clz(F) : 0;
   const int reach = (int)lane - start;
   double I = f ? acc : pre;
+  // only as many steps as the longest window needs (rows spanning few
+  // lanes: one or two); a step whose distance exceeds every lane's reach
+  // adds nothing, so the sums are the same bits as with all five steps
+  const int maxreach = (int)__reduce_max_sync(FULL, (unsigned)reach);
 #pragma unroll
   for (int d = 1; d < 32; d <<= 1) {
+    if (d > maxreach) break;
     const double u = __shfl_up_sync(FULL, I, d);
     if (reach >= d) I += u;
   }
