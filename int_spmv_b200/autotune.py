@@ -7,7 +7,7 @@ fastest.  The candidates vary:
   with plain loads or bulk-copy staging, tile columns, or row-parallel;
 - the kernel variant: slots per lane (the vector width: 8 or 16 for
   stream_wide, 2 or 4 for stream_ldg), prefetch depth or bulk-copy stages,
-  warps per SM (threads per tile) and shared-memory x bands;
+  warps per SM (threads per tile) and a per-CTA x window in shared memory;
 - the segment size;
 - for SpMM, the right-hand sides per pass (the RHS block).
 
@@ -37,7 +37,6 @@ SPMV_CANDIDATES = [
     ("COM128", dict(kernel="wide", variant=8)),   # 16 slots per lane, 8192-slot segments
     ("COM128", dict(kernel="wide", variant=9)),   # 16 slots per lane, 2048-slot segments
     ("COM128", dict(kernel="wide", variant=11)),  # bulk-copy staged, 16 slots per lane
-    ("COM128", dict(kernel="wide", variant=7)),   # 8 slots per lane, shared-memory x band
     ("COM128", dict(kernel="wide", variant=16)),  # 8 slots per lane, x gathered through the texture pipe
     ("COM128", dict(kernel="wide", variant=26)),  # 8 slots per lane, per-CTA x window by one bulk copy
     ("COM128", dict(kernel="wide", variant=32)),  # 8 slots per lane, next batch's columns loaded ahead
@@ -49,7 +48,6 @@ SPMV_CANDIDATES = [
     ("COM128", dict(kernel="ldg", variant=0)),
     ("COM128", dict(kernel="ldg", variant=2)),
     ("COM128", dict(kernel="ldg", variant=12)),
-    ("COM128", dict(kernel="ldg", variant=8)),
     ("COM128", dict(kernel="tma", variant=0)),
     ("COM128", dict(kernel="ldg", variant=2, units_per_warp=1024)),
     ("NOC1", dict(kernel="ldg", variant=2)),

@@ -223,119 +223,40 @@ size_t seg_slots_of(const ispmv_plan_s *p, size_t upu) {
   return std::max(SS, ((size_t)p->opts.units_per_warp * upu + SS - 1) / SS * SS);
 }
 
-// x-window kernel variants: (warps per CTA, shared doubles per CTA, segment slots)
-struct XwCfg { int warps; UIN cap; size_t seg; };
-bool xw_variant(int v, XwCfg *c) {
-  switch (v) {
-    case 8: *c = {16, 4096, 1024}; return true;
-    case 9: *c = {16, 8192, 1024}; return true;
-    case 10: *c = {8, 2048, 1024}; return true;
-    case 11: *c = {16, 6144, 2048}; return true;
-    case 17: *c = {16, 4096, 1024}; return true;  // lean gathers (stream_xw2)
-    case 18: *c = {16, 8192, 2048}; return true;
-    case 19: *c = {8, 4096, 2048}; return true;
-    case 20: *c = {16, 12288, 2048}; return true;
-    default: return false;
-  }
-}
-
-// stream_wide variants: slots per lane; x bands in shared memory (plain
-// loads only) and shared doubles for them; segment slots; CTAs per SM the
-// registers are sized for (plain loads); rows through a per-warp buffer
-// (coalesced y stores) or written by the lane that ends them; and for the
-// staged form (tma) the stages per warp and warps per CTA.
+// stream_wide variants, numbered as measured (numbers not listed here were
+// measured and retired: x bands in shared memory, per-warp row buffers,
+// other segment sizes, stage counts and window sizes; see the design notes):
+// slots per lane, per-CTA x window (cap doubles), segment slots, CTAs per SM
+// the registers are sized for (plain loads), and for the staged form (tma)
+// the stages per warp and warps per CTA.
 struct WideCfg {
-  int spl; bool win; UIN cap; size_t seg; int minb; bool buf; bool tma; int stages; int warps; bool tex = false;
+  int spl; UIN cap; size_t seg; int minb; bool tma; int stages; int warps; bool tex = false;
   bool tmem = false;  // stream staged through tensor memory (stream_tmem); stages = TMEM stages,
                       // warps = consumer warps per CTA (4 per column half)
   bool stg = false;   // one x window per CTA (cap doubles), chosen at plan time, copied by one bulk copy
   bool pfc = false;   // the next batch's columns loaded one batch ahead
+  bool ok = true;     // a variant this build runs
 };
 constexpr int WIDE_WARPS = 8;
 WideCfg wide_variant(int v) {
   switch (v) {
-    case 1: return {16, false, 0, 4096, 3, true, false, 0, 8};
-    case 2: return {16, true, 6144, 4096, 2, false, false, 0, 8};
-    case 3: return {16, true, 6144, 4096, 2, true, false, 0, 8};
-    case 4: return {8, false, 0, 2048, 4, false, false, 0, 8};
-    case 5: return {8, false, 0, 2048, 4, true, false, 0, 8};
-    case 6: return {16, true, 4096, 2048, 2, false, false, 0, 8};
-    case 7: return {8, true, 4096, 4096, 4, false, false, 0, 8};
-    case 8: return {16, false, 0, 8192, 3, false, false, 0, 8};
-    case 9: return {16, false, 0, 2048, 3, false, false, 0, 8};
-    case 10: return {8, false, 0, 4096, 0, false, true, 3, 8};
-    case 11: return {16, false, 0, 4096, 0, false, true, 2, 4};
-    case 12: return {16, false, 0, 4096, 0, false, true, 3, 4};
-    case 13: return {8, false, 0, 4096, 0, false, true, 4, 4};
-    case 14: return {16, false, 0, 4096, 2, false, false, 0, 8};
-    case 15: return {16, false, 0, 8192, 2, false, false, 0, 8};
-    case 16: return {8, false, 0, 2048, 4, false, false, 0, 8, true};   // texture gathers
-    case 17: return {16, false, 0, 4096, 3, false, false, 0, 8, true};
-    case 18: return {8, false, 0, 8192, 0, false, false, 4, 4, false, true};   // TMEM-staged stream
-    case 19: return {16, false, 0, 8192, 0, false, false, 2, 4, false, true};
-    case 20: return {8, false, 0, 8192, 0, false, false, 2, 8, false, true};
-    case 21: return {16, false, 0, 8192, 0, false, false, 2, 8, false, true};
-    // x bands sized for a CTA span of about 800-1600 rows plus a band of
-    // +/-1000 or more: the near half of a band-split plan
-    case 22: return {8, true, 4096, 1024, 4, false, false, 0, 8};
-    case 23: return {8, true, 6144, 2048, 4, false, false, 0, 8};
-    // a per-CTA x window (the densest interval of the CTA's columns) copied
-    // into shared memory by one bulk copy
-    case 24: return {8, false, 4096, 1024, 4, false, false, 0, 8, false, false, true};
-    case 25: return {8, false, 6144, 2048, 4, false, false, 0, 8, false, false, true};
-    case 26: return {8, false, 3072, 1024, 4, false, false, 0, 8, false, false, true};
-    case 27: return {16, false, 6144, 2048, 3, false, false, 0, 8, false, false, true};
-    case 28: return {8, false, 2048, 512, 4, false, false, 0, 8, false, false, true};
-    case 29: return {8, false, 3072, 512, 4, false, false, 0, 8, false, false, true};
-    case 30: return {8, false, 2560, 1024, 4, false, false, 0, 8, false, false, true};
-    // the next batch's columns loaded one batch ahead, with and without the
-    // per-CTA x window, at 4 and 3 CTAs per SM
-    case 31: return {8, false, 3072, 1024, 4, false, false, 0, 8, false, false, true, true};
-    case 32: return {8, false, 0, 2048, 4, false, false, 0, 8, false, false, false, true};
-    case 33: return {8, false, 0, 2048, 3, false, false, 0, 8, false, false, false, true};
-    case 34: return {8, false, 3072, 1024, 3, false, false, 0, 8, false, false, true, true};
-    default: return {16, false, 0, 4096, 3, false, false, 0, 8};
-  }
-}
-
-// Picks up to 3 diagonal bands (offset, half-width) of col - row from a
-// deterministic sample of the nonzeros: the densest interval that fits the
-// budget, then the densest of what is left, while a band holds >= 5% of the
-// sample.  `span` is the typical row range of one CTA.
-void choose_windows(const str_matCSR *csr, UIN cap, double span, sss::XWin *xw) {
-  xw->nwin = 0;
-  const size_t nnz = csr->nnz, S = std::min<size_t>(nnz, 1u << 21);
-  if (!S) return;
-  std::vector<long long> d(S);
-  const double stride = (double)nnz / (double)S;
-  for (size_t i = 0, r = 0; i < S; i++) {
-    const size_t j = (size_t)(i * stride);
-    while (csr->row[r + 1] <= j) r++;
-    d[i] = (long long)csr->col[j] - (long long)r;
-  }
-  std::sort(d.begin(), d.end());
-  std::vector<char> used(S, 0);
-  long long budget = (long long)cap;
-  for (int k = 0; k < sss::XW_MAX; k++) {
-    const long long hmax = (budget - (long long)span) / 2;
-    if (hmax < 1) break;
-    const long long W = 2 * hmax + 1;
-    size_t best = 0, ba = 0, bb = 0, cnt = 0;
-    for (size_t a = 0, b = 0; a < S; a++) {  // [a, b): points with d in [d[a], d[a] + W)
-      if (b < a) { b = a; cnt = 0; }
-      while (b < S && d[b] < d[a] + W) { cnt += !used[b]; b++; }
-      if (cnt > best) { best = cnt; ba = a; bb = b; }
-      cnt -= !used[a];
+    case 0: return {16, 0, 4096, 3, false, 0, 8};
+    case 4: return {8, 0, 2048, 4, false, 0, 8};
+    case 8: return {16, 0, 8192, 3, false, 0, 8};
+    case 9: return {16, 0, 2048, 3, false, 0, 8};
+    case 11: return {16, 0, 4096, 0, true, 2, 4};                            // bulk-copy staged stream
+    case 16: return {8, 0, 2048, 4, false, 0, 8, true};                      // texture gathers
+    case 18: return {8, 0, 8192, 0, false, 4, 4, false, true};               // TMEM-staged stream
+    case 19: return {16, 0, 8192, 0, false, 2, 4, false, true};
+    case 20: return {8, 0, 8192, 0, false, 2, 8, false, true};
+    case 21: return {16, 0, 8192, 0, false, 2, 8, false, true};
+    case 26: return {8, 3072, 1024, 4, false, 0, 8, false, false, true};     // per-CTA x window, one bulk copy
+    case 32: return {8, 0, 2048, 4, false, 0, 8, false, false, false, true}; // next batch's columns ahead
+    default: {
+      WideCfg c{16, 0, 4096, 3, false, 0, 8};
+      c.ok = false;
+      return c;
     }
-    if (best * 20 < S) break;
-    long long lo = d[ba], hi = d[ba];
-    for (size_t i = ba; i < bb; i++)
-      if (!used[i]) { lo = std::min(lo, d[i]); hi = std::max(hi, d[i]); used[i] = 1; }
-    const long long center = (lo + hi) / 2, half = (hi - lo + 1) / 2 + 1;
-    xw->off[xw->nwin] = center;
-    xw->half[xw->nwin] = half;
-    xw->nwin++;
-    budget -= (long long)span + 2 * half;
   }
 }
 
@@ -372,15 +293,19 @@ double random_far_fraction(const str_matCSR *csr) {
 // kernel has the registers for it); else 16 slots per lane, bulk-copy staged
 // for FP64 values with u32 columns that are not scattered (measured fastest
 // there), plain loads for scattered columns and for the FP32, lo-word and
-// 16-bit-delta forms.  An explicit variant is kept.
+// 16-bit-delta forms (FP32 values: 8192-slot segments).  An explicit variant
+// is kept.
+int auto_variant(const ispmv_plan_s *p, bool long_rows, bool scattered) {
+  const bool plain = p->opts.val_kind == ISPMV_VAL_F64 && p->opts.col_kind == ISPMV_COL_U32;
+  const bool f32 = p->opts.val_kind == ISPMV_VAL_F32;
+  if (!long_rows) return scattered && !narrow_kinds(p) ? (f32 ? 32 : 26) : 4;
+  if (plain && !scattered) return 11;
+  return f32 ? 8 : 0;  // FP32 values: 8192-slot segments (measured 3% faster on the 27-point stencil)
+}
 void auto_wide(ispmv_plan_s *p, const str_matCSR *csr) {
   p->opts.kernel = ISPMV_KERNEL_WIDE;
   if (p->opts.variant != 0) return;
-  const bool long_rows = (double)csr->nnz >= 16.0 * (double)p->n;
-  const bool plain = p->opts.val_kind == ISPMV_VAL_F64 && p->opts.col_kind == ISPMV_COL_U32;
-  const bool scattered = random_far_fraction(csr) >= 0.05;
-  const int short_scattered = p->opts.val_kind == ISPMV_VAL_F32 ? 32 : 26;
-  p->opts.variant = !long_rows ? (scattered && !narrow_kinds(p) ? short_scattered : 4) : plain && !scattered ? 11 : 0;
+  p->opts.variant = auto_variant(p, (double)csr->nnz >= 16.0 * (double)p->n, random_far_fraction(csr) >= 0.05);
 }
 
 // The per-CTA x windows of the staged stream_wide variants: CTA t walks
@@ -456,21 +381,20 @@ int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v,
     heads[q >> 5] |= 1u << (q & 31);
     rowmap.push_back(r);
   }
-  XwCfg xc;
-  bool xwv = p->opts.kernel == ISPMV_KERNEL_LDG && !narrow_kinds(p) && xw_variant(p->opts.variant, &xc);
   const bool wide = p->opts.kernel == ISPMV_KERNEL_WIDE;
+  size_t wide_seg = 0;
   if (wide) {
     const WideCfg wc = wide_variant(p->opts.variant);
     const bool lo16 = p->opts.val_kind == ISPMV_VAL_F32_LO16;
-    if ((narrow_kinds(p) && (wc.win || wc.tma || wc.buf || wc.tmem || wc.stg || wc.pfc)) || (lo16 && wc.tex))
+    if (!wc.ok) return fail(ISPMV_ERR_UNSUPPORTED, "stream_wide: no such variant");
+    if ((narrow_kinds(p) && (wc.tma || wc.tmem || wc.stg || wc.pfc)) || (lo16 && wc.tex))
       return fail(ISPMV_ERR_UNSUPPORTED,
-                  "stream_wide: 16-bit column deltas and BF16 lo-words on the plain-load variants without x bands "
+                  "stream_wide: 16-bit column deltas and BF16 lo-words on the plain-load variants "
                   "(lo-words: not the texture-gather variants)");
-    xc = {wc.warps, wc.cap, wc.seg};
-    xwv = wc.win;
+    wide_seg = wc.seg;
   }
-  p->seg_slots = xwv && p->opts.units_per_warp <= 0 ? xc.seg : seg_slots_of(p, 1);
-  if (wide && (p->opts.units_per_warp <= 0 || wide_variant(p->opts.variant).tmem)) p->seg_slots = xc.seg;
+  p->seg_slots = seg_slots_of(p, 1);
+  if (wide && (p->opts.units_per_warp <= 0 || wide_variant(p->opts.variant).tmem)) p->seg_slots = wide_seg;
   if (wide && p->seg_slots % SS) p->seg_slots = (p->seg_slots + SS - 1) / SS * SS;
   p->nseg = (p->slots_pad + p->seg_slots - 1) / p->seg_slots;
   std::vector<UIN> segh(std::max<size_t>(1, p->nseg), 0);
@@ -625,14 +549,6 @@ int setup_stream(ispmv_plan_s *p, const str_matCSR *csr, std::vector<double> &v,
   p->nrowmap = any_empty ? rowmap.size() : 0;
   const bool stg = wide && wide_variant(p->opts.variant).stg;
   if (stg) TRY(stage_windows(p, v, c));
-  if (xwv) {
-    const double rows_per_slot = (double)rowmap.size() / (double)std::max<size_t>(1, p->slots);
-    choose_windows(csr, xc.cap, rows_per_slot * (double)(xc.warps * p->seg_slots), &p->xw);
-    p->xw.cap = xc.cap;
-    p->xw.rowmap = p->rowmap;
-    p->xw.n = p->n;
-    p->xw.nrows_c = (UIN)rowmap.size();
-  }
   TRY(empty_rows(p, csr));
   TRY(alloc_records(p));
   if (stg) p->xw.status = p->status;
@@ -935,7 +851,6 @@ int dev_csr_stream(ispmv_plan_s *p, UIN n, UIN nnz, const UIN *row, const UIN *c
     p->opts.kernel = ISPMV_KERNEL_WIDE;
     if (p->opts.variant == 0) {
       const bool long_rows = (double)nnz >= 16.0 * (double)n;
-      const bool plain = p->opts.val_kind == ISPMV_VAL_F64;
       bool scattered = false;
       const size_t S = std::min<size_t>(nnz, 1u << 16);
       if (S) {
@@ -948,14 +863,12 @@ int dev_csr_stream(ispmv_plan_s *p, UIN n, UIN nnz, const UIN *row, const UIN *c
         ISPMV_TRY(cudaStreamSynchronize(s));
         scattered = (double)hfar / (double)S >= 0.05;
       }
-      const int short_scattered = p->opts.val_kind == ISPMV_VAL_F32 ? 32 : 26;
-      p->opts.variant = !long_rows ? (scattered ? short_scattered : 4) : plain && !scattered ? 11 : 0;
+      p->opts.variant = auto_variant(p, long_rows, scattered);
     }
   }
   const WideCfg wc = wide_variant(p->opts.variant);
-  if (wc.win || wc.tmem)
-    return fail(ISPMV_ERR_UNSUPPORTED,
-                "plan from a device CSR: the lane-interleaved kernel without x bands or TMEM staging");
+  if (!wc.ok || wc.tmem)
+    return fail(ISPMV_ERR_UNSUPPORTED, "plan from a device CSR: the lane-interleaved kernel without TMEM staging");
   if (wc.stg && nnz > 0x7FFFFFFFu)
     return fail(ISPMV_ERR_UNSUPPORTED, "plan from a device CSR: per-CTA x windows up to 2^31 - 1 nonzeros");
   p->fmt = F_CSR;
@@ -1345,10 +1258,11 @@ cudaTextureObject_t x_texture(ispmv_plan_s *p, const void *src, size_t bytes, bo
   return p->xtex;
 }
 
-template <typename VT, int SPL, int NW, int MINB, bool BUF, bool D16 = false, bool TEX = false, bool STG = false,
-          bool LO = false, bool PFC = false>
+template <typename VT, int SPL, int MINB, bool D16 = false, bool TEX = false, bool STG = false, bool LO = false,
+          bool PFC = false>
 int launch_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, const char *name) {
-  if constexpr (sizeof(VT) == 4 && NW == 0 && !LO) {
+  constexpr int NW = STG ? 1 : 0;
+  if constexpr (sizeof(VT) == 4 && !STG && !LO) {
     // FP32 values: gather from an FP32 copy of x (the value the FP32 multiply uses)
     if (!p->x32) TRY(dev_alloc(p, p->n, &p->x32));
     const unsigned gc = (unsigned)std::min<size_t>(((size_t)p->n / 2 + 255) / 256, (size_t)sm_count() * 8) + 1;
@@ -1356,35 +1270,31 @@ int launch_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, cons
     else wide::x_to_f32<false><<<gc, 256, 0, s>>>(p->n, x, p->x32);
     TRY(check_launch("x_to_f32"));
     const cudaTextureObject_t tx = TEX ? x_texture(p, p->x32, (size_t)p->n * 4, true) : 0;
-    if (TEX && !tx)
-      return launch_wide<VT, SPL, NW, MINB, BUF, D16, false>(p, x, o, s, "stream_wide<tex: x gathered with loads>");
-    auto *k = wide::stream_wide<VT, float, SPL, NW, WIDE_WARPS, MINB, BUF, D16, TEX, false, false, PFC>;
-    const size_t smem = (BUF ? (size_t)WIDE_WARPS * 32 * SPL : 0) * sizeof(double);
+    if (TEX && !tx) return launch_wide<VT, SPL, MINB, D16, false>(p, x, o, s, "stream_wide<tex: x gathered with loads>");
+    wide::stream_wide<VT, float, SPL, 0, WIDE_WARPS, MINB, D16, TEX, false, false, PFC>
+        <<<(unsigned)((p->nseg + WIDE_WARPS - 1) / WIDE_WARPS), WIDE_WARPS * 32, 0, s>>>(
+            p->slots, p->slots_pad, p->seg_slots, p->nseg, static_cast<const VT *>(p->val), p->col, p->heads, p->segh,
+            p->xw, p->x32, o, p->narrow, tx);
+    return check_launch(name);
+  } else {
+    const cudaTextureObject_t tx = TEX ? x_texture(p, x, (size_t)p->n * 8, false) : 0;
+    if (TEX && !tx) return launch_wide<VT, SPL, MINB, D16, false>(p, x, o, s, "stream_wide<tex: x gathered with loads>");
+    auto *k = wide::stream_wide<VT, double, SPL, NW, WIDE_WARPS, MINB, D16, TEX, STG, LO, PFC>;
+    const size_t smem = STG ? (size_t)p->xw.cap * sizeof(double) : 0;
     if (smem) ISPMV_TRY(cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<(unsigned)((p->nseg + WIDE_WARPS - 1) / WIDE_WARPS), WIDE_WARPS * 32, smem, s>>>(
-        p->slots, p->slots_pad, p->seg_slots, p->nseg, static_cast<const VT *>(p->val), p->col, p->heads, p->segh,
-        p->xw, p->x32, o, p->narrow, tx);
+    const unsigned g = (unsigned)((p->nseg + WIDE_WARPS - 1) / WIDE_WARPS);
+    k<<<g, WIDE_WARPS * 32, smem, s>>>(p->slots, p->slots_pad, p->seg_slots, p->nseg, static_cast<const VT *>(p->val),
+                                        p->col, p->heads, p->segh, p->xw, x, o, p->narrow, tx);
     return check_launch(name);
   }
-  const cudaTextureObject_t tx = TEX ? x_texture(p, x, (size_t)p->n * 8, false) : 0;
-  if (TEX && !tx)
-    return launch_wide<VT, SPL, NW, MINB, BUF, D16, false>(p, x, o, s, "stream_wide<tex: x gathered with loads>");
-  auto *k = wide::stream_wide<VT, double, SPL, NW, WIDE_WARPS, MINB, BUF, D16, TEX, STG, LO, PFC>;
-  const size_t smem =
-      ((NW ? (size_t)p->xw.cap : 0) + (BUF ? (size_t)WIDE_WARPS * 32 * SPL : 0)) * sizeof(double);
-  if (smem) ISPMV_TRY(cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  const unsigned g = (unsigned)((p->nseg + WIDE_WARPS - 1) / WIDE_WARPS);
-  k<<<g, WIDE_WARPS * 32, smem, s>>>(p->slots, p->slots_pad, p->seg_slots, p->nseg, static_cast<const VT *>(p->val),
-                                      p->col, p->heads, p->segh, p->xw, x, o, p->narrow, tx);
-  return check_launch(name);
 }
 
 // The staged form: persistent, as many CTAs as fit on the SMs (at most one
 // warp per segment).
 template <typename VT, int SPL, int STAGES, int W>
 int launch_wide_tma(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, const char *name) {
-  auto *k = wide::stream_wide_tma<VT, SPL, STAGES, W, false>;
-  const size_t smem = wide::tma_smem_bytes<VT, SPL, STAGES, W, false>();
+  auto *k = wide::stream_wide_tma<VT, SPL, STAGES, W>;
+  const size_t smem = wide::tma_smem_bytes<VT, SPL, STAGES, W>();
   ISPMV_TRY(cudaFuncSetAttribute((const void *)k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   ISPMV_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, W * 32, smem));
@@ -1419,15 +1329,6 @@ int launch_tmem(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, cons
   return check_launch(name);
 }
 
-// stream_wide<slots per lane, x bands, CTAs per SM, row buffer> for 0..3 bands.
-#define ISPMV_WIDE_NW(SPL, MINB, BUF)                                                                        \
-  switch (nw) {                                                                                              \
-    case 0: return launch_wide<VT, SPL, 0, MINB, BUF>(p, x, o, s, "stream_wide<" #SPL ",w0,b" #MINB ",buf" #BUF ">"); \
-    case 1: return launch_wide<VT, SPL, 1, MINB, BUF>(p, x, o, s, "stream_wide<" #SPL ",w1,b" #MINB ",buf" #BUF ">"); \
-    case 2: return launch_wide<VT, SPL, 2, MINB, BUF>(p, x, o, s, "stream_wide<" #SPL ",w2,b" #MINB ",buf" #BUF ">"); \
-    default: return launch_wide<VT, SPL, 3, MINB, BUF>(p, x, o, s, "stream_wide<" #SPL ",w3,b" #MINB ",buf" #BUF ">"); \
-  }
-
 template <typename VT>
 int run_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
   const WideCfg wc = wide_variant(p->opts.variant);
@@ -1439,70 +1340,34 @@ int run_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
       default: return launch_tmem<VT, 16, 2, 2>(p, x, o, s, "stream_tmem<16,s2,w8>");
     }
   }
-  if (wc.tma) {
-    switch (p->opts.variant) {
-      case 10: return launch_wide_tma<VT, 8, 3, 8>(p, x, o, s, "stream_wide_tma<8,s3,w8>");
-      case 11: return launch_wide_tma<VT, 16, 2, 4>(p, x, o, s, "stream_wide_tma<16,s2,w4>");
-      case 12: return launch_wide_tma<VT, 16, 3, 4>(p, x, o, s, "stream_wide_tma<16,s3,w4>");
-      default: return launch_wide_tma<VT, 8, 4, 4>(p, x, o, s, "stream_wide_tma<8,s4,w4>");
-    }
-  }
+  if (wc.tma) return launch_wide_tma<VT, 16, 2, 4>(p, x, o, s, "stream_wide_tma<16,s2,w4>");
+  const bool d = p->opts.col_kind == ISPMV_COL_D16;
   if constexpr (sizeof(VT) == 4) {
-    if (p->opts.val_kind == ISPMV_VAL_F32_LO16) {  // plain loads, FP64 x, no bands (setup checks)
-      const bool d = p->opts.col_kind == ISPMV_COL_D16;
+    if (p->opts.val_kind == ISPMV_VAL_F32_LO16) {  // plain loads, FP64 x (setup checks)
       if (wc.spl == 8)
-        return d ? launch_wide<VT, 8, 0, 4, false, true, false, false, true>(p, x, o, s, "stream_wide<8,w0,b4,buf0,d16,lo>")
-                 : launch_wide<VT, 8, 0, 4, false, false, false, false, true>(p, x, o, s, "stream_wide<8,w0,b4,buf0,lo>");
-      if (wc.minb == 2)
-        return d ? launch_wide<VT, 16, 0, 2, false, true, false, false, true>(p, x, o, s, "stream_wide<16,w0,b2,buf0,d16,lo>")
-                 : launch_wide<VT, 16, 0, 2, false, false, false, false, true>(p, x, o, s, "stream_wide<16,w0,b2,buf0,lo>");
-      return d ? launch_wide<VT, 16, 0, 3, false, true, false, false, true>(p, x, o, s, "stream_wide<16,w0,b3,buf0,d16,lo>")
-               : launch_wide<VT, 16, 0, 3, false, false, false, false, true>(p, x, o, s, "stream_wide<16,w0,b3,buf0,lo>");
+        return d ? launch_wide<VT, 8, 4, true, false, false, true>(p, x, o, s, "stream_wide<8,w0,b4,d16,lo>")
+                 : launch_wide<VT, 8, 4, false, false, false, true>(p, x, o, s, "stream_wide<8,w0,b4,lo>");
+      return d ? launch_wide<VT, 16, 3, true, false, false, true>(p, x, o, s, "stream_wide<16,w0,b3,d16,lo>")
+               : launch_wide<VT, 16, 3, false, false, false, true>(p, x, o, s, "stream_wide<16,w0,b3,lo>");
     }
   }
-  if (wc.pfc) {  // u32 columns (setup checks); the window where x allows the bulk copy
-    const bool win = wc.stg && (reinterpret_cast<uintptr_t>(x) & 15u) == 0;
-    if (wc.minb == 3)
-      return win ? launch_wide<VT, 8, 1, 3, false, false, false, true, false, true>(p, x, o, s, "stream_wide<8,stg,b3,pfc>")
-                 : launch_wide<VT, 8, 0, 3, false, false, false, false, false, true>(p, x, o, s, "stream_wide<8,w0,b3,pfc>");
-    return win ? launch_wide<VT, 8, 1, 4, false, false, false, true, false, true>(p, x, o, s, "stream_wide<8,stg,b4,pfc>")
-               : launch_wide<VT, 8, 0, 4, false, false, false, false, false, true>(p, x, o, s, "stream_wide<8,w0,b4,pfc>");
-  }
+  if (wc.pfc)  // u32 columns (setup checks)
+    return launch_wide<VT, 8, 4, false, false, false, false, true>(p, x, o, s, "stream_wide<8,w0,b4,pfc>");
   if (wc.stg) {
-    if ((reinterpret_cast<uintptr_t>(x) & 15u) == 0) {
-      if (wc.spl == 8) return launch_wide<VT, 8, 1, 4, false, false, false, true>(p, x, o, s, "stream_wide<8,stg,b4>");
-      return launch_wide<VT, 16, 1, 3, false, false, false, true>(p, x, o, s, "stream_wide<16,stg,b3>");
-    }
+    if ((reinterpret_cast<uintptr_t>(x) & 15u) == 0)
+      return launch_wide<VT, 8, 4, false, false, true>(p, x, o, s, "stream_wide<8,stg,b4>");
     // x not 16-byte aligned (no bulk copy): plain loads over the same stream
-    if (wc.spl == 8) return launch_wide<VT, 8, 0, 4, false>(p, x, o, s, "stream_wide<8,w0,b4,buf0>");
-    return launch_wide<VT, 16, 0, 3, false>(p, x, o, s, "stream_wide<16,w0,b3,buf0>");
+    return launch_wide<VT, 8, 4>(p, x, o, s, "stream_wide<8,w0,b4>");
   }
-  const int nw = wc.win ? std::min(std::max(p->xw.nwin, 0), 3) : 0;
-  if (wc.tex) {  // texture gathers (loads where x does not fit a texture)
-    const bool d = p->opts.col_kind == ISPMV_COL_D16;
-    if (wc.spl == 8)
-      return d ? launch_wide<VT, 8, 0, 4, false, true, true>(p, x, o, s, "stream_wide<8,w0,b4,buf0,d16,tex>")
-               : launch_wide<VT, 8, 0, 4, false, false, true>(p, x, o, s, "stream_wide<8,w0,b4,buf0,tex>");
-    return d ? launch_wide<VT, 16, 0, 3, false, true, true>(p, x, o, s, "stream_wide<16,w0,b3,buf0,d16,tex>")
-             : launch_wide<VT, 16, 0, 3, false, false, true>(p, x, o, s, "stream_wide<16,w0,b3,buf0,tex>");
-  }
-  if (p->opts.col_kind == ISPMV_COL_D16) {  // plain loads, no bands, direct row writes (setup checks)
-    if (wc.spl == 8) return launch_wide<VT, 8, 0, 4, false, true>(p, x, o, s, "stream_wide<8,w0,b4,buf0,d16>");
-    if (wc.minb == 2) return launch_wide<VT, 16, 0, 2, false, true>(p, x, o, s, "stream_wide<16,w0,b2,buf0,d16>");
-    return launch_wide<VT, 16, 0, 3, false, true>(p, x, o, s, "stream_wide<16,w0,b3,buf0,d16>");
-  }
-  if (wc.spl == 8) {
-    if (wc.buf) { ISPMV_WIDE_NW(8, 4, 1) }
-    ISPMV_WIDE_NW(8, 4, 0)
-  }
-  if (wc.minb == 2) {
-    if (wc.buf) { ISPMV_WIDE_NW(16, 2, 1) }
-    ISPMV_WIDE_NW(16, 2, 0)
-  }
-  if (wc.buf) return launch_wide<VT, 16, 0, 3, 1>(p, x, o, s, "stream_wide<16,w0,b3,buf1>");
-  return launch_wide<VT, 16, 0, 3, 0>(p, x, o, s, "stream_wide<16,w0,b3,buf0>");
+  if (wc.tex)  // texture gathers (loads where x does not fit a texture)
+    return d ? launch_wide<VT, 8, 4, true, true>(p, x, o, s, "stream_wide<8,w0,b4,d16,tex>")
+             : launch_wide<VT, 8, 4, false, true>(p, x, o, s, "stream_wide<8,w0,b4,tex>");
+  if (wc.spl == 8)
+    return d ? launch_wide<VT, 8, 4, true>(p, x, o, s, "stream_wide<8,w0,b4,d16>")
+             : launch_wide<VT, 8, 4>(p, x, o, s, "stream_wide<8,w0,b4>");
+  return d ? launch_wide<VT, 16, 3, true>(p, x, o, s, "stream_wide<16,w0,b3,d16>")
+           : launch_wide<VT, 16, 3>(p, x, o, s, "stream_wide<16,w0,b3>");
 }
-#undef ISPMV_WIDE_NW
 
 template <typename VT>
 int run_stream(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
@@ -1521,65 +1386,13 @@ int run_stream(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
       sss::stream_narrow<VT, false, true><<<g, 256, 0, s>>>(nslots, spad, sslots, nseg, val, col, heads, segh, p->narrow, x, o);
     return check_launch("stream_narrow");
   }
-  XwCfg xc;
-  if (p->opts.kernel == ISPMV_KERNEL_LDG && p->opts.variant >= 17 && xw_variant(p->opts.variant, &xc)) {
-    const size_t smem = (size_t)xc.cap * sizeof(double);
-    const unsigned g = (unsigned)((nseg + xc.warps - 1) / xc.warps);
-    const int nw = std::max(1, p->xw.nwin);
-#define ISPMV_XW2(NW, W)                                                                                       \
-  do {                                                                                                          \
-    ISPMV_TRY(cudaFuncSetAttribute((const void *)sss::stream_xw2<VT, NW, W>,                                    \
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));                    \
-    sss::stream_xw2<VT, NW, W><<<g, W * 32, smem, s>>>(nslots, spad, sslots, nseg, val, col, heads, segh, p->xw, \
-                                                       x, o);                                                   \
-    nm = "stream_xw2<" #NW "," #W ">";                                                                          \
-  } while (0)
-    const char *nm = "stream_xw2";
-    if (xc.warps == 16) {
-      if (nw == 1) ISPMV_XW2(1, 16);
-      else if (nw == 2) ISPMV_XW2(2, 16);
-      else ISPMV_XW2(3, 16);
-    } else {
-      if (nw == 1) ISPMV_XW2(1, 8);
-      else if (nw == 2) ISPMV_XW2(2, 8);
-      else ISPMV_XW2(3, 8);
-    }
-#undef ISPMV_XW2
-    return check_launch(nm);
-  }
-  if (p->opts.kernel == ISPMV_KERNEL_LDG && xw_variant(p->opts.variant, &xc)) {
-    const size_t smem = (size_t)xc.cap * sizeof(double);
-    const unsigned g = (unsigned)((nseg + xc.warps - 1) / xc.warps);
-    if (xc.warps == 16) {
-      ISPMV_TRY(cudaFuncSetAttribute((const void *)sss::stream_xw<VT, 16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
-      sss::stream_xw<VT, 16><<<g, 512, smem, s>>>(nslots, spad, sslots, nseg, val, col, heads, segh, p->xw, x, o);
-    } else {
-      ISPMV_TRY(cudaFuncSetAttribute((const void *)sss::stream_xw<VT, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)smem));
-      sss::stream_xw<VT, 8><<<g, 256, smem, s>>>(nslots, spad, sslots, nseg, val, col, heads, segh, p->xw, x, o);
-    }
-    return check_launch("stream_xw");
-  }
   if (p->opts.kernel == ISPMV_KERNEL_TMA) {
     int *status = p->status;
     void *args[] = {&nslots, &spad, &sslots, &nseg, &val, &col, &heads, &segh, (void *)&x, &o, &status};
     const int cps = p->opts.ctas_per_sm;
-    // variants: (warps per CTA, stages per warp, slots per stage); CTAs per SM from shared memory
-    switch (p->opts.variant) {
-      case 1:
-        return launch_staged_w<8>(sss::stream_tma<VT, 8, 3, 256>, sss::smem_bytes<8, 3, VT, 256>(), nseg,
-                                  cps ? cps : 3, s, "stream_tma<8,3,256>", args);
-      case 2:
-        return launch_staged_w<16>(sss::stream_tma<VT, 16, 2, 128>, sss::smem_bytes<16, 2, VT, 128>(), nseg,
-                                   cps ? cps : 4, s, "stream_tma<16,2,128>", args);
-      case 3:
-        return launch_staged_w<4>(sss::stream_tma<VT, 4, 4, 512>, sss::smem_bytes<4, 4, VT, 512>(), nseg,
-                                  cps ? cps : 2, s, "stream_tma<4,4,512>", args);
-      default:
-        return launch_staged_w<8>(sss::stream_tma<VT, 8, 2, 256>, sss::smem_bytes<8, 2, VT, 256>(), nseg,
-                                  cps ? cps : 4, s, "stream_tma<8,2,256>", args);
-    }
+    // 8 warps per CTA, 2 stages of 256 slots per warp; CTAs per SM from shared memory
+    return launch_staged_w<8>(sss::stream_tma<VT, 8, 2, 256>, sss::smem_bytes<8, 2, VT, 256>(), nseg,
+                              cps ? cps : 4, s, "stream_tma<8,2,256>", args);
   }
   if (p->opts.variant == ISPMV_VARIANT_QUEUE) {
     ISPMV_TRY(cudaMemsetAsync(p->queue, 0, sizeof(unsigned long long), s));
@@ -1602,17 +1415,8 @@ int run_stream(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
   nm = "stream_ldg<" #SPL "," #PD "," #MINB ",pf" #PF ">";                                                      \
   break
   switch (p->opts.variant) {
-    case 1: ISPMV_SSS(4, 1, 4);
     case 2: ISPMV_SSS(4, 0, 6);
-    case 3: ISPMV_SSS(2, 1, 6);
-    case 4: ISPMV_SSS(2, 0, 8);
-    case 5: ISPMV_SSS(2, 1, 5);
-    case 6: ISPMV_SSS(4, 0, 8);
-    case 7: ISPMV_SSS(2, 0, 6);
     case 12: ISPMV_SSS_PF(4, 0, 6, 2);
-    case 13: ISPMV_SSS_PF(4, 0, 6, 4);
-    case 14: ISPMV_SSS_PF(4, 0, 6, 8);
-    case 15: ISPMV_SSS_PF(4, 0, 5, 4);
     default: ISPMV_SSS(4, 0, 5);
   }
 #undef ISPMV_SSS

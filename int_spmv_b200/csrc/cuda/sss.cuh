@@ -370,202 +370,19 @@ __global__ void __launch_bounds__(256, 6) stream_queue(size_t nslots, size_t nsl
   }
 }
 
-// x windows: up to XW_MAX diagonal bands of x staged in shared memory.
-// A CTA's warps own consecutive segments, so its rows form one range
-// [r0, r1]; band k covers columns [r0 + off_k - h_k, r1 + off_k + h_k]
-// (clipped to [0, n) and to the CTA's share of shared memory).  The plan
-// picks the bands from the histogram of col - row.  A gather whose column
-// falls in a band reads shared memory; any other column reads x through
-// L1/L2, so the result does not depend on the bands.
-constexpr int XW_MAX = 3;
+// The per-CTA x windows of wide::stream_wide's staged form (STG): CTA b
+// copies x[tlo[b], tlo[b] + tlen[b]) into shared memory with one bulk copy
+// (tlo, tlen even; tlo + tlen <= n rounded down to even; tlen <= cap).  A
+// gather whose column falls in the window reads shared memory; any other
+// column reads x through L1/L2, so the result does not depend on it.
 struct XWin {
-  int nwin;
-  long long off[XW_MAX];
-  long long half[XW_MAX];
+  int nwin;            // 1 when the plan has windows, else 0
   UIN cap;             // doubles of shared memory per CTA
-  const UIN *rowmap;   // compressed -> real rows (nullptr: identity)
   UIN n;               // rows (= columns)
-  UIN nrows_c;         // compressed rows (non-empty)
-  // per-CTA windows of wide::stream_wide's staged form: CTA b copies
-  // x[tlo[b], tlo[b] + tlen[b]) into shared memory with one bulk copy
-  // (tlo, tlen even; tlo + tlen <= n rounded down to even; tlen <= cap)
   const UIN *tlo = nullptr;
   const UIN *tlen = nullptr;
   int *status = nullptr;  // ISPMV_ERR_TIMEOUT when the copy's wait gave up
 };
-
-struct WinState {
-  long long lo[XW_MAX];
-  UIN len[XW_MAX];
-  UIN base[XW_MAX];  // offset of band k in shared memory
-};
-
-__device__ __forceinline__ double xw_load(const WinState &w, int nwin, const double *sx, const FPT *__restrict__ x,
-                                          UIN c) {
-#pragma unroll
-  for (int k = 0; k < XW_MAX; k++) {
-    if (k < nwin) {
-      const long long d = (long long)c - w.lo[k];
-      if (d >= 0 && d < (long long)w.len[k]) return sx[w.base[k] + (UIN)d];
-    }
-  }
-  return __ldg(x + c);
-}
-
-template <typename VT, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, 48 / WARPS) stream_xw(size_t nslots, size_t nslots_pad, size_t seg_slots,
-                                                           size_t nseg, const VT *__restrict__ val,
-                                                           const UIN *__restrict__ col, const UIN *__restrict__ heads,
-                                                           const UIN *__restrict__ segh, XWin xw,
-                                                           const FPT *__restrict__ x, seg::Out o) {
-  constexpr int SPL = 4, BT = 128;
-  extern __shared__ __align__(16) double sx[];
-  __shared__ WinState sw;
-  const unsigned lane = threadIdx.x & 31u;
-  const size_t seg0 = (size_t)blockIdx.x * WARPS;
-  const size_t segid = seg0 + (threadIdx.x >> 5);
-  // the CTA's row range, from the start counts of its first and one-past-last segments
-  if (threadIdx.x == 0) {
-    const size_t segl = min(seg0 + WARPS, nseg);
-    UIN c0 = segh[seg0];
-    c0 = c0 > 0 ? c0 - 1 : 0;                                    // the run open at the first slot
-    UIN c1 = segl < nseg ? segh[segl] : xw.nrows_c;              // rows started before the end
-    c1 = c1 > 0 ? c1 - 1 : 0;
-    if (c1 >= xw.nrows_c) c1 = xw.nrows_c ? xw.nrows_c - 1 : 0;
-    const long long r0 = xw.rowmap ? xw.rowmap[c0] : c0, r1 = xw.rowmap ? xw.rowmap[c1] : c1;
-    UIN used = 0;
-#pragma unroll
-    for (int k = 0; k < XW_MAX; k++) {
-      long long lo = r0 + xw.off[k] - xw.half[k], hi = r1 + xw.off[k] + xw.half[k] + 1;
-      lo = lo < 0 ? 0 : lo;
-      hi = hi > (long long)xw.n ? (long long)xw.n : hi;
-      long long len = (k < xw.nwin && hi > lo) ? hi - lo : 0;
-      if (len > (long long)(xw.cap - used)) len = xw.cap - used;  // shared memory budget
-      sw.lo[k] = lo;
-      sw.len[k] = (UIN)len;
-      sw.base[k] = used;
-      used += (UIN)len;
-    }
-  }
-  __syncthreads();
-  WinState w;
-#pragma unroll
-  for (int k = 0; k < XW_MAX; k++) {
-    w.lo[k] = sw.lo[k];
-    w.len[k] = sw.len[k];
-    w.base[k] = sw.base[k];
-    for (UIN i = threadIdx.x; i < w.len[k]; i += WARPS * 32) sx[w.base[k] + i] = __ldg(x + w.lo[k] + i);
-  }
-  __syncthreads();
-  if (segid >= nseg) return;
-  const size_t s0 = segid * seg_slots;
-  const size_t s1 = min(s0 + seg_slots, nslots_pad);
-  const int nbat = (int)((s1 - s0) / BT);
-  Run st;
-  begin(st, o, segid, segh[segid], __ldg(heads + (s0 >> 5)));
-  for (int j = 0; j < nbat; j++) {
-    const size_t b = s0 + (size_t)j * BT, sl = b + SPL * lane;
-    Vals<VT, SPL> v;
-    v.get(val, sl);
-    Cols<SPL> c;
-    c.get(col, sl);
-    Words<SPL> h;
-    get_words<SPL>(h, heads, b);
-    double p[SPL];
-#pragma unroll
-    for (int k = 0; k < SPL; k++) p[k] = pk::prod<VT>(v[k], xw_load(w, xw.nwin, sx, x, c[k]));
-    if (sl + SPL > nslots) {
-#pragma unroll
-      for (int k = 0; k < SPL; k++)
-        if (sl + k >= nslots) p[k] = 0.0;
-    }
-    batch<SPL>(p, h, st, o);
-  }
-  finish(st, o);
-}
-
-// Lean x-band gathers: NW bands known at compile time, one unsigned compare
-// per band, and one generic-address load that reads shared memory for a
-// column inside a band and global memory (L1/L2) otherwise.
-template <int NW>
-__device__ __forceinline__ double xw_gather(const WinState &w, const double *sx, const FPT *__restrict__ x, UIN c) {
-  const double *src = x + c;
-#pragma unroll
-  for (int k = NW - 1; k >= 0; k--) {
-    const UIN d = c - (UIN)w.lo[k];  // band starts lie in [0, n]: the unsigned difference is exact
-    if (d < w.len[k]) src = sx + w.base[k] + d;
-  }
-  return *src;
-}
-
-template <typename VT, int NW, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32, 48 / WARPS) stream_xw2(size_t nslots, size_t nslots_pad,
-                                                                     size_t seg_slots, size_t nseg,
-                                                                     const VT *__restrict__ val,
-                                                                     const UIN *__restrict__ col,
-                                                                     const UIN *__restrict__ heads,
-                                                                     const UIN *__restrict__ segh, XWin xw,
-                                                                     const FPT *__restrict__ x, seg::Out o) {
-  constexpr int SPL = 4, BT = 128;
-  extern __shared__ __align__(16) double sx[];
-  __shared__ WinState sw;
-  const unsigned lane = threadIdx.x & 31u;
-  const size_t seg0 = (size_t)blockIdx.x * WARPS;
-  const size_t segid = seg0 + (threadIdx.x >> 5);
-  if (threadIdx.x == 0) {
-    const size_t segl = min(seg0 + WARPS, nseg);
-    UIN c0 = segh[seg0];
-    c0 = c0 > 0 ? c0 - 1 : 0;
-    UIN c1 = segl < nseg ? segh[segl] : xw.nrows_c;
-    c1 = c1 > 0 ? c1 - 1 : 0;
-    if (c1 >= xw.nrows_c) c1 = xw.nrows_c ? xw.nrows_c - 1 : 0;
-    const long long r0 = xw.rowmap ? xw.rowmap[c0] : c0, r1 = xw.rowmap ? xw.rowmap[c1] : c1;
-    UIN used = 0;
-#pragma unroll
-    for (int k = 0; k < XW_MAX; k++) {
-      long long lo = r0 + xw.off[k] - xw.half[k], hi = r1 + xw.off[k] + xw.half[k] + 1;
-      lo = lo < 0 ? 0 : lo;
-      hi = hi > (long long)xw.n ? (long long)xw.n : hi;
-      long long len = (k < NW && hi > lo) ? hi - lo : 0;
-      if (len > (long long)(xw.cap - used)) len = xw.cap - used;
-      sw.lo[k] = lo;
-      sw.len[k] = (UIN)len;
-      sw.base[k] = used;
-      used += (UIN)len;
-    }
-  }
-  __syncthreads();
-  WinState w;
-#pragma unroll
-  for (int k = 0; k < XW_MAX; k++) {
-    w.lo[k] = sw.lo[k];
-    w.len[k] = sw.len[k];
-    w.base[k] = sw.base[k];
-    for (UIN i = threadIdx.x; i < w.len[k]; i += WARPS * 32) sx[w.base[k] + i] = __ldg(x + w.lo[k] + i);
-  }
-  __syncthreads();
-  if (segid >= nseg) return;
-  const size_t s0 = segid * seg_slots;
-  const size_t s1 = min(s0 + seg_slots, nslots_pad);
-  const int nbat = (int)((s1 - s0) / BT);
-  Run st;
-  begin(st, o, segid, segh[segid], __ldg(heads + (s0 >> 5)));
-  for (int j = 0; j < nbat; j++) {
-    Slots<VT, SPL> cur;
-    cur.get(val, col, heads, s0 + (size_t)j * BT, lane);
-    const size_t sl = s0 + (size_t)j * BT + SPL * lane;
-    double p[SPL];
-#pragma unroll
-    for (int k = 0; k < SPL; k++) p[k] = pk::prod<VT>(cur.v[k], xw_gather<NW>(w, sx, x, cur.c[k]));
-    if (sl + SPL > nslots) {
-#pragma unroll
-      for (int k = 0; k < SPL; k++)
-        if (sl + k >= nslots) p[k] = 0.0;
-    }
-    batch<SPL>(p, cur.h, st, o);
-  }
-  finish(st, o);
-}
 
 // Reduced-byte streams (4 slots per lane, no prefetch, 6 CTAs/SM):
 //   LO   FP32 values plus, in segments whose rows need it, a BF16 residual

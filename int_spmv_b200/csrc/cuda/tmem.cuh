@@ -221,7 +221,7 @@ __global__ void __launch_bounds__((CW * H + 1) * 32)
         for (int k = 0; k < SPL; k++)
           if (sl + k >= nslots) xv[k] = (XT)0;
       }
-      wide::batch<VT, XT, SPL, false>(v, xv, bits, st, o, nullptr);
+      wide::batch<VT, XT, SPL>(v, xv, bits, st, o);
     }
     if (ok) sss::finish(st, o);
     else if (lane == 0) atomicExch(&failed, 1);

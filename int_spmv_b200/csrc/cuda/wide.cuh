@@ -15,16 +15,15 @@
 //     b + (k / V)*32*V + l*V + k % V with V = 16 / sizeof(element), so every
 //     vector load of the warp is 512 contiguous bytes;
 //   - gathers x through L1/L2 with plain loads; variants gather a column
-//     that falls in one of the plan's diagonal bands from shared memory, or
-//     every column through the texture pipe.  Which path serves a column
-//     does not change the result;
+//     that falls in the CTA's x window from shared memory, or every column
+//     through the texture pipe.  Which path serves a column does not change
+//     the result;
 //   - FP32-value plans gather an FP32 copy of x made once per product, and
 //     columns may be 16-bit deltas to a per-batch base (D16).
 // The row reduction is the slot stream's: rows are contiguous runs of
 // slots, row starts are bits of `heads` (slot order), a warp owns a segment
 // of slots and leaves two (row, partial) records per segment for
-// seg::fixup.  A row is written by the lane that ends it, or (BUF) through
-// a per-warp buffer in shared memory as coalesced stores.  Every row is
+// seg::fixup.  A row is written by the lane that ends it.  Every row is
 // written exactly once, without atomics, and the summation order is fixed,
 // so results are bitwise repeatable.
 //
@@ -129,16 +128,17 @@ __global__ void __launch_bounds__(256) x_to_f32(size_t n, const FPT *__restrict_
   }
 }
 
-// The bands of x a CTA stages: band k holds columns [lo[k], lo[k] + len[k])
-// at shared-memory offset lo[k] + delta[k] (u32 arithmetic, modulo 2^32).
+// The x window a CTA stages (NW = 1): columns [lo, lo + len) at shared-memory
+// offset lo + delta (u32 arithmetic, modulo 2^32).
 template <int NW>
 struct Bands {
   UIN lo[NW > 0 ? NW : 1], len[NW > 0 ? NW : 1], delta[NW > 0 ? NW : 1];
 };
 
-// x[c]: from a shared-memory band when c falls in one, else through L1/L2.
-// Two predicated loads into one register: the shared-memory load runs on
-// the lanes whose column is in a band, the global load on the others.
+// x[c]: from the shared-memory window when c falls in it, else through
+// L1/L2.  Two predicated loads into one register: the shared-memory load
+// runs on the lanes whose column is in the window, the global load on the
+// others.
 template <int NW>
 __device__ __forceinline__ double gather(const Bands<NW> &w, uint32_t sx_addr, const FPT *__restrict__ x, UIN c) {
   if constexpr (NW == 0) {
@@ -147,7 +147,7 @@ __device__ __forceinline__ double gather(const Bands<NW> &w, uint32_t sx_addr, c
     uint32_t in = 0, off = 0;
 #pragma unroll
     for (int k = 0; k < NW; k++) {
-      if (c - w.lo[k] < w.len[k]) {  // band starts lie in [0, n]: the unsigned difference is exact
+      if (c - w.lo[k] < w.len[k]) {  // window starts lie in [0, n]: the unsigned difference is exact
         in = 1;
         off = c + w.delta[k];
       }
@@ -175,16 +175,11 @@ __device__ __forceinline__ double gather(const Bands<NW> &w, uint32_t sx_addr, c
 // holds two row starts (rows longer than SPL slots), the lane pass is two
 // predicated multiply-adds per slot; otherwise the rows that end inside a
 // lane are written as they end.  Both paths add the same products in the
-// same order, so the result does not depend on the path.
-//
-// BUF: the rows the batch completes are entries e = 0 .. tot-1 of `rbuf`
-// (the warp's 32*SPL doubles), e = row - (st.rbase - 1); entry 0 is the row
-// open at the batch start, entry i the row of the batch's i-th start.  The
-// warp then stores the entries to y with coalesced stores.  !BUF: every row
-// goes to y (or to the segment's head record) from the lane that ends it.
-template <typename VT, typename XT, int SPL, bool BUF>
+// same order, so the result does not depend on the path.  Every row goes to
+// y (or to the segment's head record) from the lane that ends it.
+template <typename VT, typename XT, int SPL>
 __device__ __forceinline__ void batch(const VT (&v)[SPL], const XT (&xv)[SPL], unsigned bits, sss::Run &st,
-                                      const seg::Out &o, double *rbuf) {
+                                      const seg::Out &o) {
   const unsigned lane = threadIdx.x & 31u;
   const unsigned cnt = __popc(bits);
   // row starts before my slots (ex) and in the batch (tot): counts summed
@@ -209,22 +204,16 @@ __device__ __forceinline__ void batch(const VT (&v)[SPL], const XT (&xv)[SPL], u
       else acc = madd(v[k], xv[k], acc);
     }
   } else {
-    UIN r = rb;        // row of the run being summed, once past my first start
-    unsigned e = ex;   // its entry in rbuf, minus one before my first start
+    UIN r = rb;  // row of the run being summed, once past my first start
 #pragma unroll
     for (int k = 0; k < SPL; k++) {
       if ((bits >> k) & 1u) {
         if (k > first) {  // a row that starts and ends in this lane
-          if constexpr (BUF) {
-            rbuf[e] = acc;
-          } else {
-            seg::write_row(o, r, acc);  // never the segment's open row: it started in this segment
-            r++;
-          }
+          seg::write_row(o, r, acc);  // never the segment's open row: it started in this segment
+          r++;
         } else {
           pre = acc;
         }
-        e++;
         acc = 0.0;
       }
       acc = madd(v[k], xv[k], acc);
@@ -254,39 +243,16 @@ __device__ __forceinline__ void batch(const VT (&v)[SPL], const XT (&xv)[SPL], u
   }
   double E = __shfl_up_sync(FULL, I, 1);
   if (lane == 0) E = 0.0;
-  if constexpr (BUF) {
-    if (f) rbuf[ex] = E + pre;  // the row open at my lane's start ends at my first start
-    // entry 0 exists unless this is the segment's first batch and the
-    // segment starts at a row start
-    const bool valid0 = st.carry || st.row_a != NO_ROW;
-    st.csum = __shfl_sync(FULL, I, 31);
-    st.carry = true;
-    __syncwarp();
-    for (unsigned j = lane; j < tot; j += 32) {
-      const UIN row = st.rbase - 1u + j;
-      const double val = rbuf[j];
-      if (j == 0 && !valid0) continue;
-      if (row == st.row_a) {  // the row open at the segment's first slot: its head record
-        o.rec_row[2 * (size_t)st.seg] = row;
-        o.rec_sum[2 * (size_t)st.seg] = val;
-      } else {
-        seg::write_row(o, row, val);
-      }
-    }
-    __syncwarp();
-  } else {
-    // the run open at my lane's start ends at my first row start
-    if (f && (lane > 0 || !(bits & 1u) || st.carry)) sss::emit(o, st, rb - 1u, E + pre);
-    st.csum = __shfl_sync(FULL, I, 31);
-    st.carry = true;
-  }
+  // the run open at my lane's start ends at my first row start
+  if (f && (lane > 0 || !(bits & 1u) || st.carry)) sss::emit(o, st, rb - 1u, E + pre);
+  st.csum = __shfl_sync(FULL, I, 31);
+  st.carry = true;
   st.rbase += tot;
 }
 
 // Plain-load form.  MINB CTAs of WARPS*32 threads per SM bound the
-// registers.  NW = number of shared-memory x bands (0: every gather through
-// L1/L2).  Dynamic shared memory: xw.cap doubles of bands (NW > 0), then
-// (BUF) WARPS row buffers of 32*SPL doubles.
+// registers.  NW = 1 with STG (the CTA's x window in shared memory), else 0
+// (every gather through L1/L2).
 // D16: columns as 16-bit deltas to a per-batch base column (nw.cmeta, one
 // per batch of 32*SPL slots), lane-interleaved like the values; a batch whose
 // columns span more than 16 bits keeps its u32 columns in nw.esc (cmeta =
@@ -305,26 +271,23 @@ __device__ __forceinline__ void batch(const VT (&v)[SPL], const XT (&xv)[SPL], u
 // below 2^-45 of hi) by x in FP64, the others multiply in FP32.
 // PFC: the next batch's columns are loaded one batch ahead (u32 columns),
 // so a batch's gathers issue without waiting for its column load.
-template <typename VT, typename XT, int SPL, int NW, int WARPS, int MINB, bool BUF, bool D16 = false, bool TEX = false,
+template <typename VT, typename XT, int SPL, int NW, int WARPS, int MINB, bool D16 = false, bool TEX = false,
           bool STG = false, bool LO = false, bool PFC = false>
 __global__ void __launch_bounds__(WARPS * 32, MINB)
     stream_wide(size_t nslots, size_t nslots_pad, size_t seg_slots, size_t nseg, const VT *__restrict__ val,
                 const UIN *__restrict__ col, const UIN *__restrict__ heads, const UIN *__restrict__ segh,
                 sss::XWin xw, const XT *__restrict__ x, seg::Out o, sss::Narrow nw = {},
                 cudaTextureObject_t xtex = 0) {
-  static_assert(NW == 0 || sizeof(XT) == 8, "shared-memory x bands hold FP64 x");
-  static_assert(!(TEX && NW > 0), "texture gathers replace the shared-memory bands");
-  static_assert(!STG || (NW == 1 && !BUF), "the staged window is one band and uses all dynamic shared memory");
+  static_assert(NW == (STG ? 1 : 0), "the shared-memory window is the staged form's");
+  static_assert(!STG || sizeof(XT) == 8, "the window holds FP64 x");
   static_assert(!LO || (sizeof(VT) == 4 && sizeof(XT) == 8), "lo-words correct FP32 values against FP64 x");
   static_assert(!(PFC && D16), "column prefetch reads u32 columns");
   constexpr int BT = 32 * SPL;
   constexpr unsigned MASK = SPL == 32 ? 0xffffffffu : (1u << SPL) - 1u;
   extern __shared__ __align__(16) double sx[];
-  __shared__ sss::WinState sw;
   const unsigned lane = threadIdx.x & 31u;
   const size_t seg0 = (size_t)blockIdx.x * WARPS;
   const size_t segid = seg0 + (threadIdx.x >> 5);
-  double *rbuf = sx + (NW > 0 ? xw.cap : 0) + (size_t)(threadIdx.x >> 5) * BT;
   Bands<NW> w{};
   if constexpr (STG) {
     __shared__ uint64_t wbar;
@@ -349,43 +312,6 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
     w.lo[0] = lo;
     w.len[0] = len;
     w.delta[0] = 0u - lo;
-  } else if constexpr (NW > 0) {
-    // the CTA's row range, from the start counts of its first and
-    // one-past-last segments, and the bands of x it reads
-    if (threadIdx.x == 0) {
-      const size_t segl = min(seg0 + WARPS, nseg);
-      UIN c0 = segh[seg0];
-      c0 = c0 > 0 ? c0 - 1 : 0;  // the run open at the first slot
-      UIN c1 = segl < nseg ? segh[segl] : xw.nrows_c;
-      c1 = c1 > 0 ? c1 - 1 : 0;
-      if (c1 >= xw.nrows_c) c1 = xw.nrows_c ? xw.nrows_c - 1 : 0;
-      const long long r0 = xw.rowmap ? xw.rowmap[c0] : c0, r1 = xw.rowmap ? xw.rowmap[c1] : c1;
-      UIN used = 0;
-#pragma unroll
-      for (int k = 0; k < sss::XW_MAX; k++) {
-        long long lo = r0 + xw.off[k] - xw.half[k], hi = r1 + xw.off[k] + xw.half[k] + 1;
-        lo = lo < 0 ? 0 : lo;
-        hi = hi > (long long)xw.n ? (long long)xw.n : hi;
-        long long len = (k < xw.nwin && hi > lo) ? hi - lo : 0;
-        if (len > (long long)(xw.cap - used)) len = xw.cap - used;  // shared memory budget
-        sw.lo[k] = lo;
-        sw.len[k] = (UIN)len;
-        sw.base[k] = used;
-        used += (UIN)len;
-      }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < sss::XW_MAX; k++) {
-      const UIN lo = (UIN)sw.lo[k], len = sw.len[k], base = sw.base[k];
-      if (k < NW) {
-        w.lo[k] = lo;
-        w.len[k] = len;
-        w.delta[k] = base - lo;
-      }
-      for (UIN i = threadIdx.x; i < len; i += WARPS * 32) sx[base + i] = __ldg(x + lo + i);
-    }
-    __syncthreads();
   }
   if (segid >= nseg) return;
   const uint32_t sxa = tma::smem_addr(sx);
@@ -461,11 +387,11 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
         double vd[SPL];
 #pragma unroll
         for (int k = 0; k < SPL; k++) vd[k] = (double)vv[k] + sss::bf16_to_double((uint16_t)lw[k]);
-        batch<double, XT, SPL, BUF>(vd, xv, bits, st, o, rbuf);
+        batch<double, XT, SPL>(vd, xv, bits, st, o);
         continue;
       }
     }
-    batch<VT, XT, SPL, BUF>(vv, xv, bits, st, o, rbuf);
+    batch<VT, XT, SPL>(vv, xv, bits, st, o);
   }
   sss::finish(st, o);
 }
@@ -476,10 +402,9 @@ template <typename VT, int SPL>
 constexpr uint32_t stage_bytes() {
   return 32u * SPL * (uint32_t)sizeof(VT) + 32u * SPL * 4u + 4u * SPL;
 }
-template <typename VT, int SPL, int STAGES, int WARPS, bool BUF>
+template <typename VT, int SPL, int STAGES, int WARPS>
 constexpr size_t tma_smem_bytes() {
-  return ((WARPS * STAGES * 8 + 127) / 128) * 128 + (size_t)WARPS * STAGES * stage_bytes<VT, SPL>() +
-         (BUF ? (size_t)WARPS * 32 * SPL * sizeof(double) : 0);
+  return ((WARPS * STAGES * 8 + 127) / 128) * 128 + (size_t)WARPS * STAGES * stage_bytes<VT, SPL>();
 }
 
 // Staged form: persistent warps; warp g of G takes segments g, g + G, ...
@@ -488,7 +413,7 @@ constexpr size_t tma_smem_bytes() {
 // mbarrier.  Waits are bounded: a wait that gives up records
 // ISPMV_ERR_TIMEOUT in *status, the warp stops, and lane 0 waits (bounded)
 // for its copies still in flight before the CTA exits.
-template <typename VT, int SPL, int STAGES, int WARPS, bool BUF>
+template <typename VT, int SPL, int STAGES, int WARPS>
 __global__ void __launch_bounds__(WARPS * 32)
     stream_wide_tma(size_t nslots, size_t nslots_pad, size_t seg_slots, size_t nseg, const VT *__restrict__ val,
                     const UIN *__restrict__ col, const UIN *__restrict__ heads, const UIN *__restrict__ segh,
@@ -502,9 +427,6 @@ __global__ void __launch_bounds__(WARPS * 32)
   const unsigned lane = threadIdx.x & 31u;
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem) + wib * STAGES;
   unsigned char *ring = smem + ((WARPS * STAGES * 8 + 127) / 128) * 128 + (size_t)wib * STAGES * STB;
-  double *rbuf = reinterpret_cast<double *>(smem + ((WARPS * STAGES * 8 + 127) / 128) * 128 +
-                                            (size_t)WARPS * STAGES * STB) +
-                 (size_t)wib * BT;
   const size_t gw = (size_t)blockIdx.x * WARPS + wib, GW = (size_t)gridDim.x * WARPS;
   if (gw >= nseg) return;
   if (lane == 0) {
@@ -597,7 +519,7 @@ __global__ void __launch_bounds__(WARPS * 32)
       for (int k = 0; k < SPL; k++)
         if (sl + k >= nslots) xv[k] = 0.0;
     }
-    batch<VT, double, SPL, BUF>(v, xv, bits, st, o, rbuf);
+    batch<VT, double, SPL>(v, xv, bits, st, o);
     if (++cbat >= sss::seg_nst<BT>(cseg, seg_slots, nslots_pad)) {
       sss::finish(st, o);
       cseg += GW;

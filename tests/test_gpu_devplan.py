@@ -15,8 +15,8 @@ from paritylib import TOL_F32, TOL_F64, assert_parity
 pytestmark = pytest.mark.gpu
 
 # plain-load (4: 8 slots/lane; 0, 9: 16 slots/lane), bulk-copy staged (11), per-CTA x
-# window (26), window + column prefetch (31) and column prefetch (32) variants
-VARIANTS = [4, 0, 9, 11, 26, 31, 32]
+# window (26) and column prefetch (32) variants
+VARIANTS = [4, 0, 9, 11, 26, 32]
 
 
 def _dev(a):
