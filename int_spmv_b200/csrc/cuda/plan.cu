@@ -235,7 +235,6 @@ struct WideCfg {
                       // warps = consumer warps per CTA (4 per column half)
   bool stg = false;   // one x window per CTA (cap doubles), chosen at plan time, copied by one bulk copy
   bool pfc = false;   // the next batch's columns loaded one batch ahead
-  bool x64 = false;   // FP32 values multiply x rounded at each product, gathered as FP64 (no FP32 copy)
   bool ok = true;     // a variant this build runs
 };
 constexpr int WIDE_WARPS = 8;
@@ -253,7 +252,6 @@ WideCfg wide_variant(int v) {
     case 21: return {16, 0, 8192, 0, false, 2, 8, false, true};
     case 26: return {8, 3072, 1024, 4, false, 0, 8, false, false, true};     // per-CTA x window, one bulk copy
     case 32: return {8, 0, 2048, 4, false, 0, 8, false, false, false, true}; // next batch's columns ahead
-    case 33: return {16, 0, 8192, 3, false, 0, 8, false, false, false, false, true};  // 8 with FP64 x gathers
     default: {
       WideCfg c{16, 0, 4096, 3, false, 0, 8};
       c.ok = false;
@@ -1261,10 +1259,10 @@ cudaTextureObject_t x_texture(ispmv_plan_s *p, const void *src, size_t bytes, bo
 }
 
 template <typename VT, int SPL, int MINB, bool D16 = false, bool TEX = false, bool STG = false, bool LO = false,
-          bool PFC = false, bool X64 = false>
+          bool PFC = false>
 int launch_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, const char *name) {
   constexpr int NW = STG ? 1 : 0;
-  if constexpr (sizeof(VT) == 4 && !STG && !LO && !X64) {
+  if constexpr (sizeof(VT) == 4 && !STG && !LO) {
     // FP32 values: gather from an FP32 copy of x (the value the FP32 multiply uses)
     if (!p->x32) TRY(dev_alloc(p, p->n, &p->x32));
     const unsigned gc = (unsigned)std::min<size_t>(((size_t)p->n / 2 + 255) / 256, (size_t)sm_count() * 8) + 1;
@@ -1367,9 +1365,6 @@ int run_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s) {
   if (wc.spl == 8)
     return d ? launch_wide<VT, 8, 4, true>(p, x, o, s, "stream_wide<8,w0,b4,d16>")
              : launch_wide<VT, 8, 4>(p, x, o, s, "stream_wide<8,w0,b4>");
-  if (sizeof(VT) == 4 && wc.x64)  // FP32 values against FP64 x gathers: no FP32 copy of x per product
-    return d ? launch_wide<VT, 16, 3, true, false, false, false, false, true>(p, x, o, s, "stream_wide<16,w0,b3,d16,x64>")
-             : launch_wide<VT, 16, 3, false, false, false, false, false, true>(p, x, o, s, "stream_wide<16,w0,b3,x64>");
   return d ? launch_wide<VT, 16, 3, true>(p, x, o, s, "stream_wide<16,w0,b3,d16>")
            : launch_wide<VT, 16, 3>(p, x, o, s, "stream_wide<16,w0,b3>");
 }

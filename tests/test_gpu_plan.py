@@ -24,9 +24,8 @@ COMBOS = [("CSR", "rows"), ("CSR", "ldg"), ("CSR", "tma"), ("AXC", "rows"), ("AX
 KIDS = {"ldg": 1, "tma": 2, "rows": 3, "wide": 4}
 # the lane-interleaved kernel variants the library runs (0, 8, 9: 16 slots per
 # lane at three segment sizes; 4: 8 slots; 11: bulk-copy staged; 16: texture
-# gathers; 18-21: TMEM-staged; 26: per-CTA x window; 32: column prefetch; 33:
-# 8 with FP32 values gathering FP64 x)
-WIDE_VARIANTS = [0, 4, 8, 9, 11, 16, 18, 19, 20, 21, 26, 32, 33]
+# gathers; 18-21: TMEM-staged; 26: per-CTA x window; 32: column prefetch)
+WIDE_VARIANTS = [0, 4, 8, 9, 11, 16, 18, 19, 20, 21, 26, 32]
 
 
 @pytest.fixture(scope="module")
@@ -141,7 +140,7 @@ def test_wide_rejects_other_forms(env):
             make_plan(F, D, csr, g["x"], "COM128", kernel="wide", variant=v)
 
 
-WIDE_D16 = [0, 4, 8, 9, 16, 33]
+WIDE_D16 = [0, 4, 8, 9, 16]
 
 
 @pytest.mark.parametrize("fmt", ["COM128", "NOC1", "CSR"])
@@ -368,7 +367,7 @@ def test_wide_texture_gathers_and_fallback(env, val_kind):
     csr = F.CSR(row, col, val)
     ref, ab = orc.cf_csr(row, col, val, x), orc.abs_csr(row, col, val, x)
     tol = TOL_F64 if val_kind == "f64" else TOL_F32
-    for variant in (16,):
+    for variant in (16, 17):
         p = make_plan(F, D, csr, x, "COM128", kernel="wide", variant=variant, val=val_kind)
         y = p.spmv(torch.from_numpy(x).cuda()).cpu().numpy()
         if val_kind == "f64":
