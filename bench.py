@@ -276,6 +276,10 @@ def main(argv=None):
     ap.add_argument("--mode", default="spmv", choices=["spmv", "spmm", "batch"],
                     help="spmv: one matrix (default); spmm: Y = A X for k right-hand sides; batch: many "
                          "uneven banded matrices in one graph launch vs one plan per matrix")
+    ap.add_argument("--spmm-k", default="8,16,32", help="--mode spmm: right-hand-side counts, comma-separated")
+    ap.add_argument("--spmm-vals", default="f64,f32", help="--mode spmm: value forms, comma-separated (f64, f32)")
+    ap.add_argument("--spmm-plan", default="tuned", choices=["tuned", "com128"],
+                    help="--mode spmm: the autotuner's plan per case, or AUTO on AXT COM bs128")
     ap.add_argument("--batch-count", type=int, default=512)
     ap.add_argument("--batch-nmax", type=float, default=2e5, help="largest n of the batched matrices")
     ap.add_argument("--no-formats", action="store_true", help="skip the per-format table")
@@ -623,10 +627,10 @@ def _event_time(fn, steps: int, warmup: int) -> float:
     return e0.elapsed_time(e1) / 1e3 / steps
 
 
-def spmm_lines(steps: int, warmup: int, tuned: bool, peak: float):
+def spmm_lines(steps: int, warmup: int, tuned: bool, peak: float, ks=(8, 16, 32), vals=("f64", "f32")):
     """Y = A X on the power-law generator at n = 1,000,000 (seed 3), X n x k
-    row-major U[-1, 1], k in {8, 16, 32}, FP64 and FP32 values.  The plan is
-    the autotuner's choice (tuned) or AUTO's compacted AXT (bs 128).  Per
+    row-major U[-1, 1], k in `ks` (8, 16, 32), values in `vals` (FP64, FP32).
+    The plan is the autotuner's choice (tuned) or AUTO's compacted AXT (bs 128).  Per
     (value form, k): time, GFLOP/s, GB/s and the HBM fraction of
     nnz*(b_val + 4) + n*k*16 + 4*(n+1) (A read once, X and Y once), and the
     error of every column against the oracle.  Returns (results, launches)."""
@@ -641,8 +645,8 @@ def spmm_lines(steps: int, warmup: int, tuned: bool, peak: float):
     orc = Oracle()
     com = None if tuned else F.getFormatDataAXT(0, 128, 8, 1, "COM", csr, wl["x"])[1]
     res, launches = {}, 0
-    for val in ("f64", "f32"):
-        for k in (8, 16, 32):
+    for val in vals:
+        for k in ks:
             if tuned:
                 plan, choice = autotune.best_plan(csr, wl["x"], val=val, k=k, use_cache=False)
             else:
@@ -677,17 +681,20 @@ def main_spmm(a, rank, ws, W):
     import torch
     torch.cuda.set_device(0)
     peak, peak_src = hbm_peak()
-    res, launches = spmm_lines(a.steps, W, True, peak)
-    best = res["f64/k32"]
+    ks = tuple(int(k) for k in a.spmm_k.split(","))
+    vals = tuple(a.spmm_vals.split(","))
+    res, launches = spmm_lines(a.steps, W, a.spmm_plan == "tuned", peak, ks, vals)
+    head = f"{vals[0]}/k{max(ks)}"
+    best = res[head]
     out = {"metric": "SpMM GFLOP/s (2*nnz*k)", "value": best["gflops"], "unit": "GFLOP/s", "n_gpus": 1,
            "steps": a.steps, "warmup": W, "ms_per_step": best["ms"], "higher_is_better": True, "scaling": "weak",
-           "vs_baseline": None, "dtype": "f64", "data": "synthetic: power-law n=1,000,000 seed 3, X~U[-1,1]",
-           "config": {"workload": "spmm_powerlaw_n1M_seed3", "n": res["n"], "nnz": res["nnz"], "k": [8, 16, 32],
-                      "choice": "autotuned per (value form, k)"},
+           "vs_baseline": None, "dtype": vals[0], "data": "synthetic: power-law n=1,000,000 seed 3, X~U[-1,1]",
+           "config": {"workload": "spmm_powerlaw_n1M_seed3", "n": res["n"], "nnz": res["nnz"], "k": list(ks),
+                      "choice": "autotuned per (value form, k)" if a.spmm_plan == "tuned" else "AUTO on AXT COM bs128"},
            "gpu_launches": launches,
            "roofline": {"bound": "hbm", "achieved": best["gbs"], "peak": peak, "unit": "GB/s",
                         "frac": best["frac"], "traffic": None, "kernel": best["kernel"], "peak_source": peak_src,
-                        "note": "achieved = (nnz*(b_val+4) + n*k*16 + 4*(n+1)) / step time, FP64, k = 32"},
+                        "note": f"achieved = (nnz*(b_val+4) + n*k*16 + 4*(n+1)) / step time, {head}"},
            "results": res}
     print(json.dumps(out), flush=True)
 

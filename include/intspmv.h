@@ -402,9 +402,9 @@ typedef struct ispmv_plan_s *ispmv_plan;
 #define ISPMV_KERNEL_TMA 2   /* slot-stream kernel, 1D bulk copies (cp.async.bulk) into shared memory */
 #define ISPMV_KERNEL_ROWS 3  /* row-parallel kernel (CSR: lanes per row; AXC: 8 lanes per row; K1) */
 #define ISPMV_KERNEL_WIDE 4  /* slot-stream kernel over a lane-interleaved copy of the stream: 16 (or 8)
-                                slots per lane; variants with diagonal x bands or a per-CTA x window
-                                in shared memory (FP64/FP32 values, u32 columns), and plain-load
-                                variants that also take 16-bit column deltas and BF16 lo-words */
+                                slots per lane; variants with a per-CTA x window in shared memory
+                                (FP64/FP32 values, u32 columns), and plain-load variants that also
+                                take 16-bit column deltas and BF16 lo-words */
 #define ISPMV_VARIANT_QUEUE 16 /* slot-stream kernel as a work queue drained by persistent warps */
 
 typedef struct {
@@ -419,6 +419,11 @@ typedef struct {
                         ISPMV_VARIANT_QUEUE = persistent warps pulling segments
                         from a device work queue */
   int rhs_block;     /* SpMM right-hand sides per pass: 8, 16 or 32; 0 = by k */
+  int spmm_kernel;   /* SpMM: ISPMV_KERNEL_WIDE (four columns per lane, 32-byte X loads, the next
+                        step's loads in flight while a step is consumed; k a multiple of 4 and X
+                        32-byte aligned), ISPMV_KERNEL_LDG (two columns per lane) or
+                        ISPMV_KERNEL_AUTO (WIDE for blocks of 16 or 32 columns where it applies,
+                        else LDG) */
 } ispmv_plan_opts;
 
 void ispmv_plan_opts_default(ispmv_plan_opts *o);
@@ -477,7 +482,9 @@ int ispmv_plan_spmv(ispmv_plan p, const FPT *x, FPT *y, int beta, void *stream);
  * (queue reset, SpMV, row fix-up) for this (x, y, beta) on first use, and
  * captures again when they change.  Stream-ordered on `stream`. */
 int ispmv_plan_spmv_graph(ispmv_plan p, const FPT *x, FPT *y, int beta, void *stream);
-/* Y = A*X for k right-hand sides, X and Y row-major (n x k), FP64. */
+/* Y = A*X for k right-hand sides, X and Y row-major (n x k), FP64.
+ * ISPMV_ERR_UNSUPPORTED for spmm_kernel = ISPMV_KERNEL_WIDE when k is not a
+ * multiple of 4 or X is not 32-byte aligned. */
 int ispmv_plan_spmm(ispmv_plan p, UIN k, const FPT *X, FPT *Y, void *stream);
 /* End to end on HOST buffers: copies x in, runs the SpMV, copies y out and
  * synchronises `stream`.  Pinned host buffers give full PCIe bandwidth. */

@@ -49,7 +49,8 @@ class StrMatAXT(C.Structure):  # intSpmv_main.c:1114
 
 class PlanOpts(C.Structure):
     _fields_ = [("val_kind", C.c_int), ("col_kind", C.c_int), ("kernel", C.c_int), ("ctas_per_sm", C.c_int),
-                ("units_per_warp", C.c_int), ("lo_tol", C.c_double), ("variant", C.c_int), ("rhs_block", C.c_int)]
+                ("units_per_warp", C.c_int), ("lo_tol", C.c_double), ("variant", C.c_int), ("rhs_block", C.c_int),
+                ("spmm_kernel", C.c_int)]
 
 
 class PlanInfo(C.Structure):

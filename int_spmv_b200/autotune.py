@@ -57,9 +57,11 @@ SPMV_CANDIDATES = [
     ("AXC", dict(kernel="rows")),
     ("K1P", dict()),
 ]
-SPMM_CANDIDATES = [("COM128", dict(kernel="ldg", rhs_block=b)) for b in (8, 16, 32)] + \
-                  [("NOC1", dict(kernel="ldg", rhs_block=b)) for b in (8, 16, 32)] + \
-                  [("COM128", dict(kernel="wide", variant=4, rhs_block=b)) for b in (8, 16, 32)]
+# SpMM: plan kernel x columns per pass x four ("wide") or two ("ldg") columns per lane
+SPMM_CANDIDATES = [(fmt, dict(kw, rhs_block=b, spmm_kernel=sk))
+                   for fmt, kw in (("COM128", dict(kernel="ldg")), ("NOC1", dict(kernel="ldg")),
+                                   ("COM128", dict(kernel="wide", variant=4)))
+                   for b in (8, 16, 32) for sk in ("wide", "ldg")]
 
 
 def cache_path() -> Path:

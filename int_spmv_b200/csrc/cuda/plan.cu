@@ -183,7 +183,9 @@ int begin(const ispmv_plan_opts *o, ispmv_plan_s **out) {
   if (o) p->opts = *o;
   else ispmv_plan_opts_default(&p->opts);
   if (p->opts.val_kind < ISPMV_VAL_F64 || p->opts.val_kind > ISPMV_VAL_F32_LO16 || p->opts.col_kind < ISPMV_COL_U32 ||
-      p->opts.col_kind > ISPMV_COL_D16 || p->opts.kernel < 0 || p->opts.kernel > ISPMV_KERNEL_WIDE) {
+      p->opts.col_kind > ISPMV_COL_D16 || p->opts.kernel < 0 || p->opts.kernel > ISPMV_KERNEL_WIDE ||
+      (p->opts.spmm_kernel != ISPMV_KERNEL_AUTO && p->opts.spmm_kernel != ISPMV_KERNEL_LDG &&
+       p->opts.spmm_kernel != ISPMV_KERNEL_WIDE)) {
     delete p;
     return ISPMV_ERR_UNSUPPORTED;
   }
@@ -225,7 +227,7 @@ size_t seg_slots_of(const ispmv_plan_s *p, size_t upu) {
 
 // stream_wide variants, numbered as measured (numbers not listed here were
 // measured and retired: x bands in shared memory, per-warp row buffers,
-// other segment sizes, stage counts and window sizes; see the design notes):
+// other segment sizes, stage counts and window sizes):
 // slots per lane, per-CTA x window (cap doubles), segment slots, CTAs per SM
 // the registers are sized for (plain loads), and for the staged form (tma)
 // the stages per warp and warps per CTA.
@@ -1667,6 +1669,7 @@ int spmm_blocks(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
     mm::stream_spmm<G, W, VT><<<g, 256, 0, s>>>(p->slots, p->slots_pad, p->seg_slots, p->nseg, val, p->col,
                                                 p->heads, p->segh, X, o, il_spl(p));
     TRY(check_launch("stream_spmm"));
+    p->kname = last_launch();
     const size_t work = std::max(nrec, p->nempty) * CB;
     mm::spmm_fixup<CB><<<(unsigned)((work + 255) / 256), 256, 0, s>>>(nrec, p->mm_row, p->mm_sum, p->empty,
                                                                       p->nempty, o);
@@ -1675,12 +1678,55 @@ int spmm_blocks(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
   return ISPMV_OK;
 }
 
-// RHS block 8, 16 or 32 columns (ispmv_plan_opts.rhs_block, else by k): 4, 8
-// or 16 lanes per group with two columns per lane.
+// Four columns per lane: one pass per block of CB = 4G right-hand sides.
+template <int G, int T, int MINB, typename VT>
+int spmm_blocks4(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
+  constexpr int NG = 32 / G, CB = 4 * G;
+  const size_t nparts = p->nseg * NG, nrec = 2 * nparts;
+  if (p->mm_rows_cap < nrec) {
+    TRY(dev_alloc(p, std::max<size_t>(1, nrec), &p->mm_row));
+    p->mm_rows_cap = nrec;
+  }
+  if (p->mm_cap < nrec * CB) {
+    TRY(dev_alloc(p, std::max<size_t>(1, nrec * CB), &p->mm_sum));
+    p->mm_cap = nrec * CB;
+  }
+  const VT *val = static_cast<const VT *>(p->val);
+  for (UIN j0 = 0; j0 < k; j0 += CB) {
+    mm::Out o{Y, p->rowmap, p->mm_row, p->mm_sum, k, j0, std::min<UIN>(CB, k - j0)};
+    const unsigned g = (unsigned)((p->nseg * 32 + 255) / 256);
+    mm::stream_spmm4<G, T, MINB, VT><<<g, 256, 0, s>>>(p->slots, p->slots_pad, p->seg_slots, p->nseg, val, p->col,
+                                                       p->heads, p->segh, X, o, il_spl(p));
+    TRY(check_launch("stream_spmm4"));
+    p->kname = last_launch();
+    const size_t work = std::max(nrec, p->nempty) * CB;
+    mm::spmm_fixup<CB><<<(unsigned)((work + 255) / 256), 256, 0, s>>>(nrec, p->mm_row, p->mm_sum, p->empty,
+                                                                      p->nempty, o);
+    TRY(check_launch("spmm_fixup"));
+  }
+  return ISPMV_OK;
+}
+
+// RHS block 8, 16 or 32 columns (ispmv_plan_opts.rhs_block, else by k).
+// spmm_kernel: WIDE four columns per lane with 32-byte X loads (k a
+// multiple of 4, X 32-byte aligned); LDG two columns per lane (4, 8 or 16
+// lanes per group); AUTO the four-column form for blocks of 16 and 32
+// columns where it applies, else two (on 8-column blocks the two-column
+// form is the faster with FP64 values).
 template <typename VT>
 int spmm_run(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
   int g = p->opts.rhs_block;
   if (g != 8 && g != 16 && g != 32) g = k <= 8 ? 8 : k <= 16 ? 16 : 32;
+  const bool four_ok = (k & 3u) == 0 && (reinterpret_cast<uintptr_t>(X) & 31u) == 0;
+  const int kind = p->opts.spmm_kernel;
+  if (kind == ISPMV_KERNEL_WIDE && !four_ok)
+    return fail(ISPMV_ERR_UNSUPPORTED,
+                "ispmv_plan_spmm: four columns per lane need k a multiple of 4 and X 32-byte aligned");
+  if (four_ok && (kind == ISPMV_KERNEL_WIDE || (kind == ISPMV_KERNEL_AUTO && g > 8))) {
+    if (g == 8) return spmm_blocks4<2, 8, 2, VT>(p, k, X, Y, s);
+    if (g == 16) return spmm_blocks4<4, 4, 3, VT>(p, k, X, Y, s);
+    return spmm_blocks4<8, 8, 2, VT>(p, k, X, Y, s);
+  }
   if (g == 8) return spmm_blocks<4, 2, VT>(p, k, X, Y, s);
   if (g == 16) return spmm_blocks<8, 2, VT>(p, k, X, Y, s);
   return spmm_blocks<16, 2, VT>(p, k, X, Y, s);

@@ -171,6 +171,155 @@ __global__ void __launch_bounds__(256) stream_spmm(size_t nslots, size_t nslots_
   }
 }
 
+// 32-byte global accesses (sm_100): four consecutive doubles, the address
+// 32-byte aligned.
+__device__ __forceinline__ void ld4(const double *p, double (&d)[4]) {
+  asm volatile("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+               : "=d"(d[0]), "=d"(d[1]), "=d"(d[2]), "=d"(d[3])
+               : "l"(p));
+}
+__device__ __forceinline__ void st4(double *p, const double (&d)[4]) {
+  asm volatile("st.global.v4.f64 [%0], {%1, %2, %3, %4};" ::"l"(p), "d"(d[0]), "d"(d[1]), "d"(d[2]), "d"(d[3])
+               : "memory");
+}
+
+// Four right-hand sides per lane: a group of G lanes covers CB = 4G columns
+// (8, 16 or 32) with one 32-byte X load per lane and slot, and NG = 32 / G
+// groups per warp each walk their own part of the segment as in
+// stream_spmm.  A step takes T slots of the group; its X row pieces are
+// loaded while the step before is consumed, slot by slot, into the registers
+// that slot of the step before has just freed, so every lane keeps T loads
+// in flight all the time (not T at the start of a step and none while it is
+// consumed).  Values and columns of step s+1 are in registers during step
+// s, and those of step s+2 are loaded at its start.  Needs k and j0
+// multiples of 4 and X 32-byte aligned (kb is then a multiple of 4 too);
+// lanes past the block's last column load a piece of the block and store
+// nothing.
+template <int G, int T, int MINB, typename VT>
+__global__ void __launch_bounds__(256, MINB)
+    stream_spmm4(size_t nslots, size_t nslots_pad, size_t seg_slots, size_t nseg, const VT *__restrict__ val,
+                  const UIN *__restrict__ col, const UIN *__restrict__ heads, const UIN *__restrict__ segh,
+                  const FPT *__restrict__ X, Out o, unsigned il_spl) {
+  static_assert(T % G == 0 && T <= 32 && 32 % T == 0, "a step is whole lanes and inside one bitmap word");
+  constexpr int W = 4, NG = 32 / G, CB = G * W, R = T / G;  // R: slots per lane whose value and column it loads
+  const unsigned lane = threadIdx.x & 31u, grp = lane / G, jl = lane % G;
+  const size_t segid = ((size_t)blockIdx.x * 256 + threadIdx.x) >> 5;
+  if (segid >= nseg) return;
+  const size_t s0 = segid * seg_slots;
+  const size_t seg_end = min(s0 + seg_slots, nslots_pad);
+  const size_t part = (seg_end - s0) / NG;  // a multiple of 32
+  const size_t a = s0 + grp * part, b = a + part;
+  const size_t pid = segid * NG + grp;
+  UIN cr = segh[segid];
+  for (size_t w = s0 >> 5; w < (a >> 5); w++) cr += __popc(__ldg(heads + w));
+  const bool a_head = (__ldg(heads + (a >> 5)) & 1u) != 0;
+  const UIN row_a = a_head ? NO_ROW : cr - 1u;
+  UIN row = cr - 1u;
+  bool have = !a_head;
+  const unsigned j = jl * W;
+  const bool live = j < o.kb;  // all four columns, or none
+  const bool yvec = (reinterpret_cast<uintptr_t>(o.Y) & 31u) == 0;
+  const FPT *xb = X + o.j0 + (live ? j : o.kb - W);
+  double acc[W] = {0.0, 0.0, 0.0, 0.0};
+  if (jl == 0) {
+    o.rec_row[2 * pid] = NO_ROW;
+    o.rec_row[2 * pid + 1] = NO_ROW;
+  }
+  if (live) {
+#pragma unroll
+    for (int w = 0; w < W; w++) {
+      o.rec_sum[(2 * pid) * CB + j + w] = 0.0;
+      o.rec_sum[(2 * pid + 1) * CB + j + w] = 0.0;
+    }
+  }
+  auto put = [&](UIN r) {  // the run of row r ends: Y or the part's head record
+    if (!live) return;
+    if (r == row_a) {
+#pragma unroll
+      for (int w = 0; w < W; w++) o.rec_sum[(2 * pid) * CB + j + w] = acc[w];
+      return;
+    }
+    double *yp = o.Y + (size_t)real_row(o, r) * o.k + o.j0 + j;
+    if (yvec) {
+      st4(yp, acc);
+    } else {
+#pragma unroll
+      for (int w = 0; w < W; w++) yp[w] = acc[w];
+    }
+  };
+  auto load_step = [&](size_t c0, VT (&lv)[R], UIN (&lc)[R], UIN &lw) {
+#pragma unroll
+    for (int q = 0; q < R; q++) {
+      const size_t my = c0 + (size_t)q * G + jl;
+      lv[q] = val[il_spl ? wide::il_pos(my, il_spl, 16u / sizeof(VT)) : my];
+      lc[q] = col[il_spl ? wide::il_pos(my, il_spl, 4u) : my];
+    }
+    lw = __ldg(heads + (c0 >> 5));
+  };
+  if (a >= b) return;
+  // step s in registers: values mv, bitmap word mw, X pieces xv; step s+1:
+  // values v1, columns c1, word w1; step s+2: v2, c2, w2 (in flight)
+  VT mv[R], v1[R] = {}, v2[R] = {};
+  UIN mc[R], c1[R] = {}, c2[R] = {}, mw, w1 = 0, w2 = 0;
+  double xv[T][W];
+  load_step(a, mv, mc, mw);
+  if (a + T < b) load_step(a + T, v1, c1, w1);
+#pragma unroll
+  for (int i = 0; i < T; i++) {
+    const UIN c = __shfl_sync(FULL, mc[i / G], grp * G + i % G);
+    ld4(xb + (size_t)c * o.k, xv[i]);
+  }
+  for (size_t c0 = a; c0 < b; c0 += T) {
+    const bool more = c0 + T < b;  // the same for every group of the warp
+    if (c0 + 2 * T < b) load_step(c0 + 2 * T, v2, c2, w2);
+    if (c0 + T > nslots) {  // the stream's zero padding adds nothing, whatever X holds
+#pragma unroll
+      for (int i = 0; i < T; i++)
+        if (c0 + i >= nslots) {
+#pragma unroll
+          for (int w = 0; w < W; w++) xv[i][w] = 0.0;
+        }
+    }
+    const unsigned hs = mw >> (unsigned)(c0 & 31u);
+#pragma unroll
+    for (int i = 0; i < T; i++) {
+      const double v = (double)__shfl_sync(FULL, mv[i / G], grp * G + i % G);
+      if ((hs >> i) & 1u) {  // a row starts at slot c0 + i: the current run ends
+        if (have) {
+          put(row);
+          if (row == row_a && jl == 0) o.rec_row[2 * pid] = row;
+        }
+        row++;
+#pragma unroll
+        for (int w = 0; w < W; w++) acc[w] = 0.0;
+        have = true;
+      }
+#pragma unroll
+      for (int w = 0; w < W; w++) acc[w] = fma(v, xv[i][w], acc[w]);
+      if (more) {  // slot i of step s+1 into the registers just freed
+        const UIN c = __shfl_sync(FULL, c1[i / G], grp * G + i % G);
+        ld4(xb + (size_t)c * o.k, xv[i]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < R; q++) {
+      mv[q] = v1[q];
+      c1[q] = c2[q];
+      v1[q] = v2[q];
+    }
+    mw = w1;
+    w1 = w2;
+  }
+  if (have) {  // the run open at the part's end
+    const bool is_a = row == row_a;
+    if (jl == 0) o.rec_row[2 * pid + (is_a ? 0 : 1)] = row;
+    if (live) {
+#pragma unroll
+      for (int w = 0; w < W; w++) o.rec_sum[(2 * pid + (is_a ? 0 : 1)) * CB + j + w] = acc[w];
+    }
+  }
+}
+
 // Record i (of 2 per part) writes its row if it is that row's last record,
 // adding the row's earlier records; rows with no slot get zeros.
 template <int G>  // G = columns of one pass

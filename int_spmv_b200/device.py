@@ -93,12 +93,12 @@ KERNELS = {"auto": abi.KERNEL_AUTO, "ldg": abi.KERNEL_LDG, "tma": abi.KERNEL_TMA
 
 
 def plan_opts(val="f64", col="u32", kernel="auto", units_per_warp=0, ctas_per_sm=0, lo_tol=0.0,
-              variant=0, rhs_block=0) -> abi.PlanOpts:
+              variant=0, rhs_block=0, spmm_kernel="auto") -> abi.PlanOpts:
     o = abi.PlanOpts()
     load().ispmv_plan_opts_default(C.byref(o))
     o.val_kind, o.col_kind, o.kernel = VAL_KINDS[val], COL_KINDS[col], KERNELS[kernel]
     o.units_per_warp, o.ctas_per_sm, o.lo_tol, o.variant = units_per_warp, ctas_per_sm, lo_tol, variant
-    o.rhs_block = rhs_block
+    o.rhs_block, o.spmm_kernel = rhs_block, KERNELS[spmm_kernel]
     return o
 
 
@@ -109,9 +109,9 @@ class Plan:
 
     def __init__(self, csr: CSR, fmt: AXC | K1 | AXT | None = None, *, reorder: bool = True, val="f64", col="u32",
                  kernel="auto", units_per_warp=0, ctas_per_sm=0, lo_tol=0.0, variant=0, rhs_block=0,
-                 axi: np.ndarray | None = None):
+                 spmm_kernel="auto", axi: np.ndarray | None = None):
         lib = load()
-        o = plan_opts(val, col, kernel, units_per_warp, ctas_per_sm, lo_tol, variant, rhs_block)
+        o = plan_opts(val, col, kernel, units_per_warp, ctas_per_sm, lo_tol, variant, rhs_block, spmm_kernel)
         h = C.c_void_p()
         if fmt is None:
             check(lib.ispmv_plan_csr(C.byref(csr.c), C.byref(o), C.byref(h)), "ispmv_plan_csr")

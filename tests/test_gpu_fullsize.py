@@ -72,13 +72,14 @@ def powerlaw1m(env):
 @pytest.mark.parametrize("k", [8, 16, 32])
 @pytest.mark.parametrize("val_kind", ["f64", "f32"])
 @pytest.mark.parametrize("fmt", ["COM128", "NOC1"])
-def test_spmm_powerlaw1m_every_column(env, powerlaw1m, fmt, val_kind, k):
+@pytest.mark.parametrize("spmm_kernel", ["wide", "ldg"])
+def test_spmm_powerlaw1m_every_column(env, powerlaw1m, fmt, val_kind, k, spmm_kernel):
     torch, D, F, orc = env
     from test_gpu_plan import make_plan
     row, col, val, csr = powerlaw1m
     n = csr.n
     X = np.random.default_rng(3).uniform(-1, 1, (n, k))
-    p = make_plan(F, D, csr, X[:, 0], fmt, kernel="ldg", rhs_block=k, val=val_kind)
+    p = make_plan(F, D, csr, X[:, 0], fmt, kernel="ldg", rhs_block=k, val=val_kind, spmm_kernel=spmm_kernel)
     Y = torch.full((n, k), 7.0, dtype=torch.float64, device="cuda")
     p.spmm(torch.from_numpy(X).cuda(), Y)
     Yh = Y.cpu().numpy()
