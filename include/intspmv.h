@@ -420,7 +420,7 @@ typedef struct {
                         from a device work queue */
   int rhs_block;     /* SpMM right-hand sides per pass: 8, 16 or 32; 0 = by k */
   int spmm_kernel;   /* SpMM: ISPMV_KERNEL_WIDE (four columns per lane, 32-byte X loads, the next
-                        step's loads in flight while a step is consumed; k a multiple of 4 and X
+                        step's loads in flight while a step is consumed; k a multiple of 4, X and Y
                         32-byte aligned), ISPMV_KERNEL_LDG (two columns per lane) or
                         ISPMV_KERNEL_AUTO (WIDE for blocks of 16 or 32 columns where it applies,
                         else LDG) */
@@ -484,7 +484,7 @@ int ispmv_plan_spmv(ispmv_plan p, const FPT *x, FPT *y, int beta, void *stream);
 int ispmv_plan_spmv_graph(ispmv_plan p, const FPT *x, FPT *y, int beta, void *stream);
 /* Y = A*X for k right-hand sides, X and Y row-major (n x k), FP64.
  * ISPMV_ERR_UNSUPPORTED for spmm_kernel = ISPMV_KERNEL_WIDE when k is not a
- * multiple of 4 or X is not 32-byte aligned. */
+ * multiple of 4 or X or Y is not 32-byte aligned. */
 int ispmv_plan_spmm(ispmv_plan p, UIN k, const FPT *X, FPT *Y, void *stream);
 /* End to end on HOST buffers: copies x in, runs the SpMV, copies y out and
  * synchronises `stream`.  Pinned host buffers give full PCIe bandwidth. */

@@ -1650,7 +1650,7 @@ bool tmem_plan(const ispmv_plan_s *p) {
 
 // One pass per block of CB = G*W right-hand sides (G lanes per group, W
 // columns per lane).
-template <int G, int W, typename VT>
+template <int G, int W, typename VT, int SPL>
 int spmm_blocks(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
   constexpr int NG = 32 / G, CB = G * W;
   const size_t nparts = p->nseg * NG, nrec = 2 * nparts;
@@ -1666,8 +1666,8 @@ int spmm_blocks(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
   for (UIN j0 = 0; j0 < k; j0 += CB) {
     mm::Out o{Y, p->rowmap, p->mm_row, p->mm_sum, k, j0, std::min<UIN>(CB, k - j0)};
     const unsigned g = (unsigned)((p->nseg * 32 + 255) / 256);
-    mm::stream_spmm<G, W, VT><<<g, 256, 0, s>>>(p->slots, p->slots_pad, p->seg_slots, p->nseg, val, p->col,
-                                                p->heads, p->segh, X, o, il_spl(p));
+    mm::stream_spmm<G, W, VT, SPL><<<g, 256, 0, s>>>(p->slots, p->slots_pad, p->seg_slots, p->nseg, val, p->col,
+                                                     p->heads, p->segh, X, o);
     TRY(check_launch("stream_spmm"));
     p->kname = last_launch();
     const size_t work = std::max(nrec, p->nempty) * CB;
@@ -1679,7 +1679,7 @@ int spmm_blocks(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
 }
 
 // Four columns per lane: one pass per block of CB = 4G right-hand sides.
-template <int G, int T, int MINB, typename VT>
+template <int G, int T, int MINB, typename VT, int SPL>
 int spmm_blocks4(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
   constexpr int NG = 32 / G, CB = 4 * G;
   const size_t nparts = p->nseg * NG, nrec = 2 * nparts;
@@ -1695,8 +1695,8 @@ int spmm_blocks4(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
   for (UIN j0 = 0; j0 < k; j0 += CB) {
     mm::Out o{Y, p->rowmap, p->mm_row, p->mm_sum, k, j0, std::min<UIN>(CB, k - j0)};
     const unsigned g = (unsigned)((p->nseg * 32 + 255) / 256);
-    mm::stream_spmm4<G, T, MINB, VT><<<g, 256, 0, s>>>(p->slots, p->slots_pad, p->seg_slots, p->nseg, val, p->col,
-                                                       p->heads, p->segh, X, o, il_spl(p));
+    mm::stream_spmm4<G, T, MINB, VT, SPL><<<g, 256, 0, s>>>(p->slots, p->slots_pad, p->seg_slots, p->nseg, val,
+                                                            p->col, p->heads, p->segh, X, o);
     TRY(check_launch("stream_spmm4"));
     p->kname = last_launch();
     const size_t work = std::max(nrec, p->nempty) * CB;
@@ -1709,27 +1709,39 @@ int spmm_blocks4(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
 
 // RHS block 8, 16 or 32 columns (ispmv_plan_opts.rhs_block, else by k).
 // spmm_kernel: WIDE four columns per lane with 32-byte X loads (k a
-// multiple of 4, X 32-byte aligned); LDG two columns per lane (4, 8 or 16
+// multiple of 4, X and Y 32-byte aligned); LDG two columns per lane (4, 8 or 16
 // lanes per group); AUTO the four-column form for blocks of 16 and 32
 // columns where it applies, else two (on 8-column blocks the two-column
 // form is the faster with FP64 values).
-template <typename VT>
-int spmm_run(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
+template <typename VT, int SPL>
+int spmm_run_spl(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
   int g = p->opts.rhs_block;
   if (g != 8 && g != 16 && g != 32) g = k <= 8 ? 8 : k <= 16 ? 16 : 32;
-  const bool four_ok = (k & 3u) == 0 && (reinterpret_cast<uintptr_t>(X) & 31u) == 0;
+  const bool four_ok = (k & 3u) == 0 && ((reinterpret_cast<uintptr_t>(X) | reinterpret_cast<uintptr_t>(Y)) & 31u) == 0;
   const int kind = p->opts.spmm_kernel;
   if (kind == ISPMV_KERNEL_WIDE && !four_ok)
     return fail(ISPMV_ERR_UNSUPPORTED,
-                "ispmv_plan_spmm: four columns per lane need k a multiple of 4 and X 32-byte aligned");
+                "ispmv_plan_spmm: four columns per lane need k a multiple of 4 and X, Y 32-byte aligned");
   if (four_ok && (kind == ISPMV_KERNEL_WIDE || (kind == ISPMV_KERNEL_AUTO && g > 8))) {
-    if (g == 8) return spmm_blocks4<2, 8, 2, VT>(p, k, X, Y, s);
-    if (g == 16) return spmm_blocks4<4, 4, 3, VT>(p, k, X, Y, s);
-    return spmm_blocks4<8, 8, 2, VT>(p, k, X, Y, s);
+    if (g == 8) return spmm_blocks4<2, 8, 2, VT, SPL>(p, k, X, Y, s);
+    if (g == 16) return spmm_blocks4<4, 4, 3, VT, SPL>(p, k, X, Y, s);
+    return spmm_blocks4<8, 8, 2, VT, SPL>(p, k, X, Y, s);
   }
-  if (g == 8) return spmm_blocks<4, 2, VT>(p, k, X, Y, s);
-  if (g == 16) return spmm_blocks<8, 2, VT>(p, k, X, Y, s);
-  return spmm_blocks<16, 2, VT>(p, k, X, Y, s);
+  if (g == 8) return spmm_blocks<4, 2, VT, SPL>(p, k, X, Y, s);
+  if (g == 16) return spmm_blocks<8, 2, VT, SPL>(p, k, X, Y, s);
+  return spmm_blocks<16, 2, VT, SPL>(p, k, X, Y, s);
+}
+
+// The plan's stream layout as a template argument: slot order, or lane-
+// interleaved with 8 or 16 slots per lane.
+template <typename VT>
+int spmm_run(ispmv_plan_s *p, UIN k, const FPT *X, FPT *Y, cudaStream_t s) {
+  switch (il_spl(p)) {
+    case 0: return spmm_run_spl<VT, 0>(p, k, X, Y, s);
+    case 8: return spmm_run_spl<VT, 8>(p, k, X, Y, s);
+    case 16: return spmm_run_spl<VT, 16>(p, k, X, Y, s);
+    default: return fail(ISPMV_ERR_UNSUPPORTED, "ispmv_plan_spmm: lane-interleaved plans of 8 or 16 slots per lane");
+  }
 }
 }  // namespace
 

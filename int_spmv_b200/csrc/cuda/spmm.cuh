@@ -10,9 +10,9 @@
 // Row starts come from the
 // stream's bitmap; a row that ends inside the group's part is written to Y
 // directly, the runs open at the part's two ends become G-wide records that
-// spmm_fixup adds per row.  Deterministic, no atomics.  `il_spl` > 0 reads
-// a plan whose values and columns are stored lane-interleaved for
-// stream_wide (wide::il_pos with il_spl slots per lane).
+// spmm_fixup adds per row.  Deterministic, no atomics.  SPL > 0 reads a
+// plan whose values and columns are stored lane-interleaved for stream_wide
+// (wide::il_pos_c with SPL slots per lane); SPL = 0 a plan in slot order.
 #pragma once
 #include "wide.cuh"
 
@@ -29,6 +29,11 @@ struct Out {
 
 __device__ __forceinline__ UIN real_row(const Out &o, UIN r) { return o.rowmap ? o.rowmap[r] : r; }
 
+template <bool B>
+struct BoolC {
+  static constexpr bool value = B;
+};
+
 // G lanes per group, W (1 or 2) consecutive right-hand sides per lane: a
 // pass covers CB = G*W columns.  A step of the group covers T = G slots:
 // each lane loads one slot's value and column (coalesced), one step ahead
@@ -39,11 +44,11 @@ __device__ __forceinline__ UIN real_row(const Out &o, UIN r) { return o.rowmap ?
 // are handled and the products accumulated.  The loads of a step are thus in
 // flight together, ahead of the stores that row ends make to Y, and the
 // values and columns of the next step arrive meanwhile.
-template <int G, int W, typename VT>
+template <int G, int W, typename VT, int SPL>
 __global__ void __launch_bounds__(256) stream_spmm(size_t nslots, size_t nslots_pad, size_t seg_slots, size_t nseg,
                                                    const VT *__restrict__ val, const UIN *__restrict__ col,
                                                    const UIN *__restrict__ heads, const UIN *__restrict__ segh,
-                                                   const FPT *__restrict__ X, Out o, unsigned il_spl) {
+                                                   const FPT *__restrict__ X, Out o) {
   static_assert(W == 1 || W == 2, "one or two right-hand sides per lane");
   constexpr int NG = 32 / G;            // groups per warp = parts per segment
   constexpr int CB = G * W;             // columns of one pass
@@ -102,8 +107,8 @@ __global__ void __launch_bounds__(256) stream_spmm(size_t nslots, size_t nslots_
 #pragma unroll
     for (int q = 0; q < R; q++) {
       const size_t my = c0 + (size_t)q * G + jl;
-      nv[q] = val[il_spl ? wide::il_pos(my, il_spl, 16u / sizeof(VT)) : my];
-      nc[q] = col[il_spl ? wide::il_pos(my, il_spl, 4u) : my];
+      nv[q] = val[wide::il_pos_c<SPL, 16u / sizeof(VT)>(my)];
+      nc[q] = col[wide::il_pos_c<SPL, 4u>(my)];
     }
     nhw = __ldg(heads + (c0 >> 5));
   };
@@ -192,14 +197,15 @@ __device__ __forceinline__ void st4(double *p, const double (&d)[4]) {
 // in flight all the time (not T at the start of a step and none while it is
 // consumed).  Values and columns of step s+1 are in registers during step
 // s, and those of step s+2 are loaded at its start.  Needs k and j0
-// multiples of 4 and X 32-byte aligned (kb is then a multiple of 4 too);
-// lanes past the block's last column load a piece of the block and store
-// nothing.
-template <int G, int T, int MINB, typename VT>
+// multiples of 4 and X and Y 32-byte aligned (kb is then a multiple of 4
+// too); lanes past the block's last column load a piece of the block and
+// store nothing.  The last step of a part is compiled apart (no loads for a
+// next step), so a slot costs no test for it.
+template <int G, int T, int MINB, typename VT, int SPL>
 __global__ void __launch_bounds__(256, MINB)
     stream_spmm4(size_t nslots, size_t nslots_pad, size_t seg_slots, size_t nseg, const VT *__restrict__ val,
-                  const UIN *__restrict__ col, const UIN *__restrict__ heads, const UIN *__restrict__ segh,
-                  const FPT *__restrict__ X, Out o, unsigned il_spl) {
+                 const UIN *__restrict__ col, const UIN *__restrict__ heads, const UIN *__restrict__ segh,
+                 const FPT *__restrict__ X, Out o) {
   static_assert(T % G == 0 && T <= 32 && 32 % T == 0, "a step is whole lanes and inside one bitmap word");
   constexpr int W = 4, NG = 32 / G, CB = G * W, R = T / G;  // R: slots per lane whose value and column it loads
   const unsigned lane = threadIdx.x & 31u, grp = lane / G, jl = lane % G;
@@ -218,7 +224,6 @@ __global__ void __launch_bounds__(256, MINB)
   bool have = !a_head;
   const unsigned j = jl * W;
   const bool live = j < o.kb;  // all four columns, or none
-  const bool yvec = (reinterpret_cast<uintptr_t>(o.Y) & 31u) == 0;
   const FPT *xb = X + o.j0 + (live ? j : o.kb - W);
   double acc[W] = {0.0, 0.0, 0.0, 0.0};
   if (jl == 0) {
@@ -232,27 +237,12 @@ __global__ void __launch_bounds__(256, MINB)
       o.rec_sum[(2 * pid + 1) * CB + j + w] = 0.0;
     }
   }
-  auto put = [&](UIN r) {  // the run of row r ends: Y or the part's head record
-    if (!live) return;
-    if (r == row_a) {
-#pragma unroll
-      for (int w = 0; w < W; w++) o.rec_sum[(2 * pid) * CB + j + w] = acc[w];
-      return;
-    }
-    double *yp = o.Y + (size_t)real_row(o, r) * o.k + o.j0 + j;
-    if (yvec) {
-      st4(yp, acc);
-    } else {
-#pragma unroll
-      for (int w = 0; w < W; w++) yp[w] = acc[w];
-    }
-  };
   auto load_step = [&](size_t c0, VT (&lv)[R], UIN (&lc)[R], UIN &lw) {
 #pragma unroll
     for (int q = 0; q < R; q++) {
       const size_t my = c0 + (size_t)q * G + jl;
-      lv[q] = val[il_spl ? wide::il_pos(my, il_spl, 16u / sizeof(VT)) : my];
-      lc[q] = col[il_spl ? wide::il_pos(my, il_spl, 4u) : my];
+      lv[q] = val[wide::il_pos_c<SPL, 16u / sizeof(VT)>(my)];
+      lc[q] = col[wide::il_pos_c<SPL, 4u>(my)];
     }
     lw = __ldg(heads + (c0 >> 5));
   };
@@ -269,8 +259,12 @@ __global__ void __launch_bounds__(256, MINB)
     const UIN c = __shfl_sync(FULL, mc[i / G], grp * G + i % G);
     ld4(xb + (size_t)c * o.k, xv[i]);
   }
-  for (size_t c0 = a; c0 < b; c0 += T) {
-    const bool more = c0 + T < b;  // the same for every group of the warp
+  // a run that ends is stored to its Y row, or to the part's head record
+  // when it is the row open at the part's start (a select, not a branch);
+  // lanes past the block's last column store nothing
+  double *const head = o.rec_sum + (2 * pid) * CB + j;
+  auto step = [&](size_t c0, auto more_c) {
+    constexpr bool MORE = decltype(more_c)::value;  // step s+1 exists: load its X pieces
     if (c0 + 2 * T < b) load_step(c0 + 2 * T, v2, c2, w2);
     if (c0 + T > nslots) {  // the stream's zero padding adds nothing, whatever X holds
 #pragma unroll
@@ -284,11 +278,11 @@ __global__ void __launch_bounds__(256, MINB)
 #pragma unroll
     for (int i = 0; i < T; i++) {
       const double v = (double)__shfl_sync(FULL, mv[i / G], grp * G + i % G);
-      if ((hs >> i) & 1u) {  // a row starts at slot c0 + i: the current run ends
-        if (have) {
-          put(row);
-          if (row == row_a && jl == 0) o.rec_row[2 * pid] = row;
-        }
+      if (hs & (1u << i)) {  // a row starts at slot c0 + i: the current run ends
+        const bool is_a = row == row_a;
+        double *dst = is_a ? head : o.Y + (size_t)real_row(o, row) * o.k + o.j0 + j;
+        if (have && live) st4(dst, acc);
+        if (have && is_a && jl == 0) o.rec_row[2 * pid] = row;
         row++;
 #pragma unroll
         for (int w = 0; w < W; w++) acc[w] = 0.0;
@@ -296,7 +290,7 @@ __global__ void __launch_bounds__(256, MINB)
       }
 #pragma unroll
       for (int w = 0; w < W; w++) acc[w] = fma(v, xv[i][w], acc[w]);
-      if (more) {  // slot i of step s+1 into the registers just freed
+      if constexpr (MORE) {  // slot i of step s+1 into the registers just freed
         const UIN c = __shfl_sync(FULL, c1[i / G], grp * G + i % G);
         ld4(xb + (size_t)c * o.k, xv[i]);
       }
@@ -309,7 +303,10 @@ __global__ void __launch_bounds__(256, MINB)
     }
     mw = w1;
     w1 = w2;
-  }
+  };
+  size_t c0 = a;
+  for (; c0 + T < b; c0 += T) step(c0, BoolC<true>{});
+  step(c0, BoolC<false>{});
   if (have) {  // the run open at the part's end
     const bool is_a = row == row_a;
     if (jl == 0) o.rec_row[2 * pid + (is_a ? 0 : 1)] = row;

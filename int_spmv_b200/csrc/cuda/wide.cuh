@@ -47,6 +47,20 @@ __host__ __device__ inline size_t il_pos(size_t s, unsigned spl, unsigned v) {
   return b + (size_t)(k / v) * 32u * v + (size_t)l * v + k % v;
 }
 
+// il_pos with the slots per lane (0: slot order, 8 or 16) and the elements
+// per vector load known at compile time: shifts and masks, no division.
+template <int SPL, unsigned V>
+__device__ __forceinline__ size_t il_pos_c(size_t s) {
+  if constexpr (SPL == 0) {
+    return s;
+  } else {
+    static_assert((SPL & (SPL - 1)) == 0 && (V & (V - 1)) == 0, "powers of two");
+    constexpr size_t BT = 32u * SPL;
+    const unsigned r = (unsigned)(s & (BT - 1)), l = r / SPL, k = r % SPL;
+    return (s & ~(BT - 1)) + (size_t)(k / V) * 32u * V + (size_t)l * V + k % V;
+  }
+}
+
 template <typename VT, int SPL>
 struct Vals;
 template <int SPL>

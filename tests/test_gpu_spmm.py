@@ -119,10 +119,9 @@ def test_spmm_rhs_blocks_and_odd_k(env, k, rhs_block, spmm_kernel):
 
 
 def test_spmm_wide_repeatable_and_rejects(env):
-    """The four-column form gives the same bits on every run, writes Y rows
-    that are not 32-byte aligned with scalar stores, and a plan that asks
-    for it explicitly rejects k not a multiple of 4 and an X that is not
-    32-byte aligned."""
+    """The four-column form gives the same bits on every run, and a plan
+    that asks for it explicitly rejects k not a multiple of 4 and an X or Y
+    that is not 32-byte aligned (AUTO then runs the two-column form)."""
     torch, D, F, orc = env
     from int_spmv_b200 import IntSpmvError
     from int_spmv_b200 import matrices as M
@@ -136,8 +135,12 @@ def test_spmm_wide_repeatable_and_rejects(env):
     assert p.kernel_name() == "stream_spmm4"
     assert torch.equal(Y1, Y2)
     Yb = torch.full((n * 32 + 1,), 9.0, dtype=torch.float64, device="cuda")
-    p.spmm(X, Yb[1:].view(n, 32))  # Y 8 bytes into its buffer
-    assert torch.equal(Yb[1:].view(n, 32), Y1)
+    with pytest.raises(IntSpmvError):
+        p.spmm(X, Yb[1:].view(n, 32))  # Y 8 bytes into its buffer
+    pa = make_plan(F, D, csr, Xh[:, 0], "COM128", kernel="wide")
+    pa.spmm(X, Yb[1:].view(n, 32))
+    assert pa.kernel_name() == "stream_spmm"
+    assert torch.allclose(Yb[1:].view(n, 32), Y1, rtol=0, atol=1e-12)
     for j in range(32):
         xj = np.ascontiguousarray(Xh[:, j])
         assert_parity(Y1[:, j].cpu().numpy(), orc.cf_csr(row, col, val, xj), orc.abs_csr(row, col, val, xj),
