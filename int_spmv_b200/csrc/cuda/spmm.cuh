@@ -34,6 +34,13 @@ struct BoolC {
   static constexpr bool value = B;
 };
 
+// One slot of a step as the group reads it from shared memory: its value
+// and the column of the slot at the same place in the next step.
+struct alignas(16) SlotRec {
+  double v;
+  UIN c, pad;
+};
+
 // G lanes per group, W (1 or 2) consecutive right-hand sides per lane: a
 // pass covers CB = G*W columns.  A step of the group covers T = G slots:
 // each lane loads one slot's value and column (coalesced), one step ahead
@@ -196,7 +203,9 @@ __device__ __forceinline__ void st4(double *p, const double (&d)[4]) {
 // that slot of the step before has just freed, so every lane keeps T loads
 // in flight all the time (not T at the start of a step and none while it is
 // consumed).  Values and columns of step s+1 are in registers during step
-// s, and those of step s+2 are loaded at its start.  Needs k and j0
+// s, and those of step s+2 are loaded at its start; at a step's start each
+// lane writes its slots' values and next columns to the warp's records in
+// shared memory, which the group then reads as broadcasts.  Needs k and j0
 // multiples of 4 and X and Y 32-byte aligned (kb is then a multiple of 4
 // too); lanes past the block's last column load a piece of the block and
 // store nothing.  The last step of a part is compiled apart (no loads for a
@@ -263,8 +272,18 @@ __global__ void __launch_bounds__(256, MINB)
   // when it is the row open at the part's start (a select, not a branch);
   // lanes past the block's last column store nothing
   double *const head = o.rec_sum + (2 * pid) * CB + j;
+  // the warp's slot records: group g's slot i at g * (T + 1) + i (one
+  // record of padding per group, so the groups' broadcasts fall in
+  // different banks)
+  constexpr int RS = T + 1;
+  __shared__ SlotRec recs[8][NG * RS];
+  SlotRec *const wrec = recs[threadIdx.x >> 5];
+  const SlotRec *const grec = wrec + grp * RS;
   auto step = [&](size_t c0, auto more_c) {
     constexpr bool MORE = decltype(more_c)::value;  // step s+1 exists: load its X pieces
+#pragma unroll
+    for (int q = 0; q < R; q++) wrec[grp * RS + q * G + jl] = SlotRec{(double)mv[q], c1[q], 0u};
+    __syncwarp();
     if (c0 + 2 * T < b) load_step(c0 + 2 * T, v2, c2, w2);
     if (c0 + T > nslots) {  // the stream's zero padding adds nothing, whatever X holds
 #pragma unroll
@@ -277,7 +296,8 @@ __global__ void __launch_bounds__(256, MINB)
     const unsigned hs = mw >> (unsigned)(c0 & 31u);
 #pragma unroll
     for (int i = 0; i < T; i++) {
-      const double v = (double)__shfl_sync(FULL, mv[i / G], grp * G + i % G);
+      const SlotRec sr = grec[i];
+      const double v = sr.v;
       if (hs & (1u << i)) {  // a row starts at slot c0 + i: the current run ends
         const bool is_a = row == row_a;
         double *dst = is_a ? head : o.Y + (size_t)real_row(o, row) * o.k + o.j0 + j;
@@ -290,11 +310,9 @@ __global__ void __launch_bounds__(256, MINB)
       }
 #pragma unroll
       for (int w = 0; w < W; w++) acc[w] = fma(v, xv[i][w], acc[w]);
-      if constexpr (MORE) {  // slot i of step s+1 into the registers just freed
-        const UIN c = __shfl_sync(FULL, c1[i / G], grp * G + i % G);
-        ld4(xb + (size_t)c * o.k, xv[i]);
-      }
+      if constexpr (MORE) ld4(xb + (size_t)sr.c * o.k, xv[i]);  // slot i of step s+1, into the registers just freed
     }
+    __syncwarp();  // every lane has read the records before the next step writes them
 #pragma unroll
     for (int q = 0; q < R; q++) {
       mv[q] = v1[q];
