@@ -1476,12 +1476,25 @@ int run(ispmv_plan_s *p, const FPT *x, FPT *y, int beta, cudaStream_t s) {
   p->kname = last_launch();
   // the kernels after the main one (the row fix-up, K1's reorder)
   if (p->path == P_STREAM || p->path == P_UNITS) {
+    // a programmatic dependent launch when nothing (a timing event) sits
+    // between the main kernel and the fix-up in the stream
+    const bool pdl = !p->tcap || p->capturing;
     TRY(tmark(p, s, 1));
     const size_t nrec = p->slots ? 2 * p->nseg : 0;
     const size_t work = std::max(nrec, p->nempty);
     if (work) {
-      seg::fixup<<<(unsigned)((work + 255) / 256), 256, 0, s>>>(nrec, p->rec_row, p->rec_sum, p->rowmap, p->empty,
-                                                                p->nempty, y, beta);
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3((unsigned)((work + 255) / 256));
+      cfg.blockDim = dim3(256);
+      cfg.dynamicSmemBytes = 0;
+      cfg.stream = s;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      at[0].val.programmaticStreamSerializationAllowed = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = pdl ? 1 : 0;
+      ISPMV_TRY(cudaLaunchKernelEx(&cfg, seg::fixup, nrec, (const UIN *)p->rec_row, (const double *)p->rec_sum,
+                                   (const UIN *)p->rowmap, (const UIN *)p->empty, p->nempty, y, beta));
       return check_launch("fixup");
     }
     return ISPMV_OK;

@@ -93,10 +93,15 @@ __device__ __forceinline__ void finish(const State &st, const Out &o, size_t seg
 
 // Fix-up: record i writes its row if it is the row's last record, adding the
 // row's earlier records (walking back).  Also zeroes (beta = 0) the rows
-// that own no slot at all (rows of length 0).
+// that own no slot at all (rows of length 0).  Launched as a programmatic
+// dependent of the main kernel where the stream allows it, so its launch
+// overlaps the main kernel's last CTAs: griddepcontrol.wait then blocks until
+// the main kernel has completed and its records and rows are visible (it
+// returns at once for an ordinary launch).
 __global__ void fixup(size_t nrec, const UIN *__restrict__ rec_row, const double *__restrict__ rec_sum,
                       const UIN *__restrict__ rowmap, const UIN *__restrict__ empty, size_t nempty,
                       FPT *__restrict__ y, int beta) {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < nempty && !beta) y[empty[i]] = 0.0;
   if (i >= nrec) return;

@@ -302,6 +302,9 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
   constexpr int BT = 32 * SPL;
   constexpr unsigned MASK = SPL == 32 ? 0xffffffffu : (1u << SPL) - 1u;
   extern __shared__ __align__(16) double sx[];
+  // the row fix-up that follows may launch now: it waits (griddepcontrol.wait)
+  // for this grid to complete before it reads anything
+  asm volatile("griddepcontrol.launch_dependents;");
   const unsigned lane = threadIdx.x & 31u;
   const size_t seg0 = (size_t)blockIdx.x * WARPS;
   const size_t segid = seg0 + (threadIdx.x >> 5);
