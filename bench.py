@@ -335,13 +335,22 @@ def main(argv=None):
     sampler.start()
     time.sleep(0.3)
     sec, (tw0, tw1) = timed(lambda: plan.spmv(x, y), a.steps, W, ws, stream, dev)
-    # the same K steps again with an event pair around each main kernel: the
-    # dominant kernel's average launch duration for the roofline
+    # the same K steps again with an event pair around each main kernel
     plan.time_kernels(a.steps)
-    sec_k, (_, tw2) = timed(lambda: plan.spmv(x, y), a.steps, 3, ws, stream, dev)
+    sec_k, _ = timed(lambda: plan.spmv(x, y), a.steps, 3, ws, stream, dev)
     kms, klaunches = plan.kernel_ms()
     plan.time_kernels(0)
-    kern_s = max_over_ranks(kms / 1e3 / max(klaunches, 1), ws, dev)
+    kern_ev_s = max_over_ranks(kms / 1e3 / max(klaunches, 1), ws, dev)
+    # the dominant kernel's average launch duration for the roofline: K
+    # launches of the main kernel back to back between one event pair (an
+    # event pair around each launch adds the event records' gaps to every
+    # launch), after 3 untimed ones; then one product restores y
+    barrier(ws)
+    plan.time_main(x, y, 3)
+    kern_s = max_over_ranks(plan.time_main(x, y, a.steps) / 1e3, ws, dev)
+    tw2 = time.time()
+    plan.spmv(x, y)
+    torch.cuda.synchronize()
     time.sleep(0.25)
     sampler.stop()
     clocks = sampler.summary(tw0, tw2)
@@ -400,13 +409,11 @@ def main(argv=None):
             k = max(20, min(a.steps, 400))
             s_, _ = timed(lambda: p.spmv(x, y), k, 5, ws, stream, dev)
             t = s_ / k
-            # the main kernel alone (event pairs); for K1 the rest of the step
-            # is the reorder pass, the reference's ordTime (intSpmv_main.c:1001-1016)
-            p.time_kernels(k)
-            timed(lambda: p.spmv(x, y), k, 3, ws, stream, dev)
-            kms_, kn_ = p.kernel_ms()
-            p.time_kernels(0)
-            tk = kms_ / 1e3 / max(kn_, 1)
+            # the main kernel alone (k launches back to back); for K1 the rest
+            # of the step is the reorder pass, the reference's ordTime
+            # (intSpmv_main.c:1001-1016)
+            p.time_main(x, y, 3)
+            tk = max_over_ranks(p.time_main(x, y, k) / 1e3, ws, dev)
             bb = p.info["alg_bytes"]
             kid = {0: "auto", 1: "ldg", 2: "tma", 3: "rows", 4: "wide"}.get(p.info["kernel"], "?")
             row_ = {"ms": t * 1e3, "gflops": flops / t / 1e9, "gbs": bb / t / 1e9, "frac": bb / t / 1e9 / peak,
@@ -528,11 +535,14 @@ def main(argv=None):
             "gb_per_s": gbs,
             "roofline": {"bound": "hbm", "achieved": kern_gbs, "peak": peak, "unit": "GB/s",
                          "frac": kern_gbs / peak, "traffic": traffic_for(f"{wl['name']}/{a.format}/{kname}"),
-                         "kernel": kname, "kernel_ms": kern_s * 1e3, "kernel_launches": klaunches,
+                         "kernel": kname, "kernel_ms": kern_s * 1e3, "kernel_launches": a.steps,
+                         "kernel_ms_event_pairs": kern_ev_s * 1e3, "event_pair_launches": klaunches,
                          "step_gbs": gbs, "step_frac": gbs / peak, "peak_source": peak_src,
                          "note": "achieved = algorithmic bytes of one SpMV (nnz*(b_val+b_idx) + n*16 + 4*(n+1)) / the main "
-                                 "kernel's mean CUDA-event duration over K launches; step_gbs uses the whole "
-                                 "step (main kernel + row fix-up)"},
+                                 "kernel's mean duration over K launches back to back between one CUDA event pair "
+                                 "(ispmv_plan_time_main); kernel_ms_event_pairs is the mean of an event pair around "
+                                 "each main kernel inside K whole steps; step_gbs uses the whole step (main kernel + "
+                                 "row fix-up, a programmatic dependent launch)"},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(round(per_step * a.steps)),
@@ -582,11 +592,8 @@ def precision_lines(a, rank, ws, stream, dev, peak):
     for vk, ck, key, kw in forms:
         p = D.Plan(csr, com, val=vk, col=ck, **kw)
         s_, _ = timed(lambda: p.spmv(x, y), k, 5, ws, stream, dev)
-        p.time_kernels(k)
-        timed(lambda: p.spmv(x, y), k, 3, ws, stream, dev)
-        kms, kn = p.kernel_ms()
-        p.time_kernels(0)
-        t, tk = s_ / k, kms / 1e3 / max(kn, 1)
+        p.time_main(x, y, 3)
+        t, tk = s_ / k, max_over_ranks(p.time_main(x, y, k) / 1e3, ws, dev)
         bb = p.info["alg_bytes"]
         row = {"ms": t * 1e3, "kernel_ms": tk * 1e3, "gflops": 2.0 * csr.nnz / t / 1e9, "alg_bytes": bb,
                "gbs": bb / tk / 1e9, "frac": bb / tk / 1e9 / peak, "kernel": p.kernel_name(),

@@ -504,6 +504,14 @@ int ispmv_plan_status(ispmv_plan p);
  * it after the stream is synchronised. */
 int ispmv_plan_time_kernels(ispmv_plan p, int pairs);
 int ispmv_plan_kernel_ms(ispmv_plan p, double *total_ms, int *launches);
+/* The main kernel alone, timed: `reps` launches of the product's main kernel
+ * (for FP32-value plans on the lane-interleaved kernel, with the rounding of
+ * x to FP32 that precedes it) back to back on `stream` between one CUDA
+ * event pair, without the row fix-up or K1's reorder; *ms = the mean per
+ * launch.  Synchronises `stream`.  y is left without the fix-up's rows: an
+ * ispmv_plan_spmv gives the product.  Unlike an event pair around each
+ * launch, the timing holds no event record between consecutive launches. */
+int ispmv_plan_time_main(ispmv_plan p, const FPT *x, FPT *y, int reps, void *stream, double *ms);
 /* Name of the main kernel the plan's latest product launched (a static
  * string, "" before the first product), e.g. "stream_ldg<4,0,5>". */
 const char *ispmv_plan_kernel_name(ispmv_plan p);

@@ -158,6 +158,7 @@ PROTOTYPES: dict[str, tuple] = {
     "ispmv_plan_status": (C.c_int, [VP]),
     "ispmv_plan_time_kernels": (C.c_int, [VP, C.c_int]),
     "ispmv_plan_kernel_ms": (C.c_int, [VP, C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+    "ispmv_plan_time_main": (C.c_int, [VP, VP, VP, C.c_int, VP, C.POINTER(C.c_double)]),
     "ispmv_plan_kernel_name": (C.c_char_p, [VP]),
     # library facts
     "ispmv_version": (C.c_char_p, []),

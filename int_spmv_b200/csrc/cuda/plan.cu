@@ -252,7 +252,7 @@ WideCfg wide_variant(int v) {
     case 19: return {16, 0, 8192, 0, false, 2, 4, false, true};
     case 20: return {8, 0, 8192, 0, false, 2, 8, false, true};
     case 21: return {16, 0, 8192, 0, false, 2, 8, false, true};
-    case 26: return {8, 3072, 1024, 4, false, 0, 8, false, false, true};     // per-CTA x window, one bulk copy
+    case 26: return {8, 3584, 1536, 4, false, 0, 8, false, false, true};     // per-CTA x window, one bulk copy
     case 32: return {8, 0, 2048, 4, false, 0, 8, false, false, false, true}; // next batch's columns ahead
     default: {
       WideCfg c{16, 0, 4096, 3, false, 0, 8};
@@ -1626,6 +1626,27 @@ ISPMV_API int ispmv_plan_kernel_ms(ispmv_plan p, double *total_ms, int *launches
   *launches = (int)m;
   p->tcount = 0;
   return ISPMV_OK;
+}
+
+ISPMV_API int ispmv_plan_time_main(ispmv_plan p, const FPT *x, FPT *y, int reps, void *stream, double *ms) {
+  if (!p || !x || !y || reps < 1 || !ms) return ISPMV_ERR_ARG;
+  if (p->capturing) return fail(ISPMV_ERR_ARG, "ispmv_plan_time_main: not inside a graph capture");
+  cudaStream_t s = as_stream(stream);
+  auto ck = [](cudaError_t e, const char *where) { return e == cudaSuccess ? ISPMV_OK : cuda_status(e, where); };
+  cudaEvent_t e[2] = {nullptr, nullptr};
+  ISPMV_TRY(cudaEventCreate(&e[0]));
+  int st = ck(cudaEventCreate(&e[1]), "cudaEventCreate");
+  if (!st) st = ck(cudaEventRecord(e[0], s), "cudaEventRecord");
+  for (int i = 0; i < reps && !st; i++)
+    st = p->opts.val_kind == ISPMV_VAL_F64 ? run_main<double>(p, x, y, 0, s) : run_main<float>(p, x, y, 0, s);
+  if (!st) st = ck(cudaEventRecord(e[1], s), "cudaEventRecord");
+  if (!st) st = ck(cudaEventSynchronize(e[1]), "cudaEventSynchronize");
+  float t = 0.f;
+  if (!st) st = ck(cudaEventElapsedTime(&t, e[0], e[1]), "cudaEventElapsedTime");
+  for (cudaEvent_t ev : e)
+    if (ev) cudaEventDestroy(ev);
+  if (!st) *ms = (double)t / reps;
+  return st;
 }
 
 ISPMV_API const char *ispmv_plan_kernel_name(ispmv_plan p) { return p ? p->kname : ""; }

@@ -202,6 +202,17 @@ class Plan:
         check(load().ispmv_plan_kernel_ms(self._h, C.byref(ms), C.byref(n)), "ispmv_plan_kernel_ms")
         return ms.value, n.value
 
+    def time_main(self, x: torch.Tensor, y: torch.Tensor, reps: int, stream=None) -> float:
+        """Mean milliseconds of the main kernel over `reps` back-to-back
+        launches between one CUDA event pair (ispmv_plan_time_main); y is
+        left without the row fix-up (run spmv for the product)."""
+        if x.dtype != torch.float64 or x.numel() != self.n or y.numel() != self.n:
+            raise ValueError("x and y must be float64 CUDA tensors of n entries")
+        ms = C.c_double()
+        check(load().ispmv_plan_time_main(self._h, _ptr(x), _ptr(y), int(reps), _stream(stream), C.byref(ms)),
+              "ispmv_plan_time_main")
+        return ms.value
+
     def kernel_name(self) -> str:
         """The main kernel of the latest product (e.g. "stream_ldg<4,0,5>")."""
         return load().ispmv_plan_kernel_name(self._h).decode()

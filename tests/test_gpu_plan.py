@@ -245,6 +245,28 @@ def test_deterministic_and_host_e2e(env, fmt, kernel):
     assert np.array_equal(hy.numpy(), a)
 
 
+@pytest.mark.parametrize("fmt,kernel,val_kind", [("COM128", "auto", "f64"), ("COM128", "auto", "f32"),
+                                                 ("K1", "auto", "f64"), ("NOC4", "ldg", "f64")])
+def test_time_main(env, fmt, kernel, val_kind):
+    """ispmv_plan_time_main: a positive mean time for the main kernel alone;
+    it rejects a bad repetition count, and a product after it is the oracle's
+    (the timing leaves the fix-up rows out of y, spmv puts them back)."""
+    torch, D, F, orc = env
+    from int_spmv_b200 import matrices as M
+    from int_spmv_b200._lib import IntSpmvError
+    row, col, val = M.random_csr(30000, 6, rl_max=90, empty_frac=0.05)
+    x = M.uniform_x(30000, 6)
+    p, xt = check_plan(env, row, col, val, x, fmt, val_kind=val_kind, kernel=kernel)
+    y = torch.empty(30000, dtype=torch.float64, device="cuda")
+    ms = p.time_main(xt, y, 5)
+    assert 0.0 < ms < 1e3
+    with pytest.raises(IntSpmvError):
+        p.time_main(xt, y, 0)
+    p.spmv(xt, y)
+    assert_parity(y.cpu().numpy(), orc.cf_csr(row, col, val, x), orc.abs_csr(row, col, val, x),
+                  TOL_F64 if val_kind == "f64" else TOL_F32, what=f"after time_main {fmt}/{val_kind}")
+
+
 @pytest.fixture(scope="module")
 def poisson512(env):
     from int_spmv_b200 import matrices as M
