@@ -34,6 +34,13 @@ int sm_count();
   } while (0)
 
 // ---- device side --------------------------------------------------------
+// Programmatic dependent launch: a main kernel lets the launch that follows
+// it in the stream (the row fix-up, K1's reorder) start now; that kernel
+// waits (pdl_wait) for the whole main grid and its writes before it reads
+// anything.  Both are no-ops for ordinary launches.
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Inclusive segmented sum over the 32 lanes of a warp.  `head` marks the
 // first lane of each run; lanes of one run end up holding the running sum
 // from the run's head to themselves.

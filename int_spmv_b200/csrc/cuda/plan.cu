@@ -1475,10 +1475,13 @@ int run(ispmv_plan_s *p, const FPT *x, FPT *y, int beta, cudaStream_t s) {
   if (st) return st;
   p->kname = last_launch();
   // the kernels after the main one (the row fix-up, K1's reorder)
+  // the kernel after the main one is a programmatic dependent launch when
+  // nothing (a timing event) sits between the two in the stream
+  const bool pdl = !p->tcap || p->capturing;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
   if (p->path == P_STREAM || p->path == P_UNITS) {
-    // a programmatic dependent launch when nothing (a timing event) sits
-    // between the main kernel and the fix-up in the stream
-    const bool pdl = !p->tcap || p->capturing;
     TRY(tmark(p, s, 1));
     const size_t nrec = p->slots ? 2 * p->nseg : 0;
     const size_t work = std::max(nrec, p->nempty);
@@ -1488,9 +1491,6 @@ int run(ispmv_plan_s *p, const FPT *x, FPT *y, int beta, cudaStream_t s) {
       cfg.blockDim = dim3(256);
       cfg.dynamicSmemBytes = 0;
       cfg.stream = s;
-      cudaLaunchAttribute at[1];
-      at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-      at[0].val.programmaticStreamSerializationAllowed = 1;
       cfg.attrs = at;
       cfg.numAttrs = pdl ? 1 : 0;
       ISPMV_TRY(cudaLaunchKernelEx(&cfg, seg::fixup, nrec, (const UIN *)p->rec_row, (const double *)p->rec_sum,
@@ -1501,7 +1501,14 @@ int run(ispmv_plan_s *p, const FPT *x, FPT *y, int beta, cudaStream_t s) {
   }
   if (p->path == P_K1 && p->fmt != F_K1P) {
     TRY(tmark(p, s, 1));
-    pk::k1_order<<<(unsigned)((p->n + 255) / 256), 256, 0, s>>>(p->n, p->permi, p->res, y, beta);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)((p->n + 255) / 256));
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cfg.attrs = at;
+    cfg.numAttrs = pdl ? 1 : 0;
+    ISPMV_TRY(cudaLaunchKernelEx(&cfg, pk::k1_order, p->n, (const UIN *)p->permi, (const FPT *)p->res, y, beta));
     return check_launch("k1_order");
   }
   return tmark(p, s, 1);

@@ -120,6 +120,7 @@ __global__ void __launch_bounds__(TPB) k1_chunks(UIN n, UIN chunkNum, UIN nlong,
                                                  const UIN *__restrict__ nmc, const UIN *__restrict__ permi,
                                                  const UIN *__restrict__ col, const VT *__restrict__ val,
                                                  const FPT *__restrict__ x, FPT *__restrict__ out, int beta) {
+  pdl_trigger();
   const unsigned lane = threadIdx.x & 31u, lane8 = lane & 7u;
   const size_t w = ((size_t)blockIdx.x * TPB + threadIdx.x) >> 5;
   size_t c;
@@ -149,8 +150,12 @@ __global__ void __launch_bounds__(TPB) k1_chunks(UIN n, UIN chunkNum, UIN nlong,
 // Warps of a K1 launch: one per long chunk, one per 4 other chunks.
 inline size_t k1_warps(UIN chunkNum, UIN nlong) { return (size_t)nlong + ((size_t)(chunkNum - nlong) + 3) / 4; }
 
+// K1's reorder (orderArrayK1): y in original row order from the chunk-order
+// result; a programmatic dependent launch of k1_chunks where the stream
+// allows it, so it first waits for that grid and its writes.
 __global__ void k1_order(UIN n, const UIN *__restrict__ permi, const FPT *__restrict__ res, FPT *__restrict__ y,
                          int beta) {
+  pdl_wait();
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) {
     const UIN r = permi[i];
@@ -167,6 +172,7 @@ template <typename VT>
 __global__ void __launch_bounds__(TPB) noc_hn(size_t nunits, size_t nseg, UIN th, UIN useg, const UIN *__restrict__ urow,
                                               const UIN *__restrict__ col, const VT *__restrict__ val,
                                               const FPT *__restrict__ x, seg::Out o) {
+  pdl_trigger();
   const unsigned lane = threadIdx.x & 31u;
   const size_t segid = ((size_t)blockIdx.x * TPB + threadIdx.x) >> 5;
   if (segid >= nseg) return;

@@ -69,6 +69,7 @@ __global__ void __launch_bounds__(WARPS * 32) nocn_tma(size_t nunits, size_t nsl
                                                        const VT *__restrict__ val, const UIN *__restrict__ col,
                                                        const UIN *__restrict__ urow, const FPT *__restrict__ x,
                                                        seg::Out o, int *status) {
+  pdl_trigger();
   using L = StageLayout<VT>;
   constexpr int UPS = SS / TH;           // units per stage
   constexpr int TPS = SS / (8 * TH);     // tiles per stage

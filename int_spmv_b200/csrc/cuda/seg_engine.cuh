@@ -101,7 +101,7 @@ __device__ __forceinline__ void finish(const State &st, const Out &o, size_t seg
 __global__ void fixup(size_t nrec, const UIN *__restrict__ rec_row, const double *__restrict__ rec_sum,
                       const UIN *__restrict__ rowmap, const UIN *__restrict__ empty, size_t nempty,
                       FPT *__restrict__ y, int beta) {
-  asm volatile("griddepcontrol.wait;" ::: "memory");
+  pdl_wait();
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < nempty && !beta) y[empty[i]] = 0.0;
   if (i >= nrec) return;

@@ -282,6 +282,7 @@ __global__ void __launch_bounds__(256, MINB) stream_ldg(size_t nslots, size_t ns
                                                         const UIN *__restrict__ col, const UIN *__restrict__ heads,
                                                         const UIN *__restrict__ segh, const FPT *__restrict__ x,
                                                         seg::Out o) {
+  pdl_trigger();
   constexpr int BT = 32 * SPL;
   const unsigned lane = threadIdx.x & 31u;
   const size_t segid = ((size_t)blockIdx.x * 256 + threadIdx.x) >> 5;
@@ -340,6 +341,7 @@ __global__ void __launch_bounds__(256, 6) stream_queue(size_t nslots, size_t nsl
                                                        const UIN *__restrict__ col, const UIN *__restrict__ heads,
                                                        const UIN *__restrict__ segh, const FPT *__restrict__ x,
                                                        unsigned long long *queue, seg::Out o) {
+  pdl_trigger();
   constexpr int SPL = 4, BT = 128;
   const unsigned lane = threadIdx.x & 31u;
   for (;;) {
@@ -407,6 +409,7 @@ __global__ void __launch_bounds__(256, 6) stream_narrow(size_t nslots, size_t ns
                                                         const UIN *__restrict__ col, const UIN *__restrict__ heads,
                                                         const UIN *__restrict__ segh, Narrow nw,
                                                         const FPT *__restrict__ x, seg::Out o) {
+  pdl_trigger();
   constexpr int SPL = 4, BT = 128;
   const unsigned lane = threadIdx.x & 31u;
   const size_t segid = ((size_t)blockIdx.x * 256 + threadIdx.x) >> 5;
@@ -491,6 +494,7 @@ __global__ void __launch_bounds__(WARPS * 32) stream_tma(size_t nslots, size_t n
                                                          const UIN *__restrict__ col, const UIN *__restrict__ heads,
                                                          const UIN *__restrict__ segh, const FPT *__restrict__ x,
                                                          seg::Out o, int *status) {
+  pdl_trigger();
   constexpr uint32_t VB = SSZ * sizeof(VT), CB = SSZ * 4, HB = SSZ / 8, STB = VB + CB + HB;
   constexpr int NB = SSZ / BATCH;  // batches per stage
   extern __shared__ __align__(128) unsigned char smem[];

@@ -98,6 +98,7 @@ template <typename VT, typename XT, int SPL, int S, int H>
 __global__ void __launch_bounds__((CW * H + 1) * 32)
     stream_tmem(size_t nslots, size_t seg_slots, const uint32_t *__restrict__ blocks, const UIN *__restrict__ heads,
                 const UIN *__restrict__ segh, const XT *__restrict__ x, seg::Out o, int *status) {
+  pdl_trigger();
   constexpr int BT = 32 * SPL, W = words<VT, SPL>(), NCP = ncp<VT, SPL>(), NW = CW * H;
   constexpr uint32_t BB = block_bytes<VT, SPL>() * H, TCOLS = tmem_cols<VT, SPL, S, H>();
   constexpr unsigned MASK = SPL == 32 ? 0xffffffffu : (1u << SPL) - 1u;

@@ -302,9 +302,7 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
   constexpr int BT = 32 * SPL;
   constexpr unsigned MASK = SPL == 32 ? 0xffffffffu : (1u << SPL) - 1u;
   extern __shared__ __align__(16) double sx[];
-  // the row fix-up that follows may launch now: it waits (griddepcontrol.wait)
-  // for this grid to complete before it reads anything
-  asm volatile("griddepcontrol.launch_dependents;");
+  pdl_trigger();  // the row fix-up may launch now; it waits for this grid before it reads
   const unsigned lane = threadIdx.x & 31u;
   const size_t seg0 = (size_t)blockIdx.x * WARPS;
   const size_t segid = seg0 + (threadIdx.x >> 5);
@@ -448,6 +446,7 @@ __global__ void __launch_bounds__(WARPS * 32)
     stream_wide_tma(size_t nslots, size_t nslots_pad, size_t seg_slots, size_t nseg, const VT *__restrict__ val,
                     const UIN *__restrict__ col, const UIN *__restrict__ heads, const UIN *__restrict__ segh,
                     const FPT *__restrict__ x, seg::Out o, int *status) {
+  pdl_trigger();
   constexpr int BT = 32 * SPL;
   constexpr unsigned MASK = SPL == 32 ? 0xffffffffu : (1u << SPL) - 1u;
   constexpr uint32_t VB = BT * sizeof(VT), CB = BT * 4, HB = BT / 8, STB = stage_bytes<VT, SPL>();
