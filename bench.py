@@ -189,6 +189,15 @@ def max_over_ranks(v: float, ws: int, device=None) -> float:
     return float(t.item())
 
 
+def rest(ws: int, seconds: float = 1.5):
+    """Drain the device, idle `seconds`, then meet the other ranks: a
+    measurement that follows starts from a rested GPU."""
+    import torch
+    torch.cuda.synchronize()
+    time.sleep(seconds)
+    barrier(ws)
+
+
 def barrier(ws: int):
     if ws > 1:
         import torch.distributed as dist
@@ -345,8 +354,11 @@ def main(argv=None):
     # chunks of at least max(K, 200)/5 launches of the main kernel back to
     # back, each between one event pair (an event pair around each launch
     # adds the event records' gaps to every launch), after 3 untimed ones;
-    # the median chunk, every chunk reported; then one product restores y
-    barrier(ws)
+    # the median chunk, every chunk reported; then one product restores y.
+    # Measured from a rested GPU, as the HBM peak (a best-of-10 copy) is: on
+    # these boxes ~100 ms of back-to-back HBM-bound work slows this kernel by
+    # up to 8%, and ~2 s idle restores it
+    rest(ws)
     plan.time_main(x, y, 3)
     per_chunk = max(20, max(a.steps, 200) // 5)
     chunks = [plan.time_main(x, y, per_chunk) for _ in range(5)]
@@ -412,9 +424,10 @@ def main(argv=None):
             k = max(20, min(a.steps, 400))
             s_, _ = timed(lambda: p.spmv(x, y), k, 5, ws, stream, dev)
             t = s_ / k
-            # the main kernel alone (k launches back to back); for K1 the rest
-            # of the step is the reorder pass, the reference's ordTime
-            # (intSpmv_main.c:1001-1016)
+            # the main kernel alone (k launches back to back, from a rested
+            # GPU); for K1 the rest of the step is the reorder pass, the
+            # reference's ordTime (intSpmv_main.c:1001-1016)
+            rest(ws, 0.5)
             p.time_main(x, y, 3)
             tk = max_over_ranks(p.time_main(x, y, k) / 1e3, ws, dev)
             bb = p.info["alg_bytes"]
@@ -544,7 +557,8 @@ def main(argv=None):
                          "step_gbs": gbs, "step_frac": gbs / peak, "peak_source": peak_src,
                          "note": "achieved = algorithmic bytes of one SpMV (nnz*(b_val+b_idx) + n*16 + 4*(n+1)) / the main "
                                  "kernel's mean duration over launches back to back between one CUDA event pair "
-                                 "(ispmv_plan_time_main), the median of 5 such chunks (kernel_ms_chunks); "
+                                 "(ispmv_plan_time_main), the median of 5 such chunks (kernel_ms_chunks), timed "
+                                 "from a rested GPU (1.5 s idle first) as the HBM peak's best-of-10 copy is; "
                                  "kernel_ms_event_pairs is the mean of an event pair around "
                                  "each main kernel inside K whole steps; step_gbs uses the whole step (main kernel + "
                                  "row fix-up, a programmatic dependent launch)"},
@@ -597,6 +611,7 @@ def precision_lines(a, rank, ws, stream, dev, peak):
     for vk, ck, key, kw in forms:
         p = D.Plan(csr, com, val=vk, col=ck, **kw)
         s_, _ = timed(lambda: p.spmv(x, y), k, 5, ws, stream, dev)
+        rest(ws, 0.5)
         p.time_main(x, y, 3)
         t, tk = s_ / k, max_over_ranks(p.time_main(x, y, k) / 1e3, ws, dev)
         bb = p.info["alg_bytes"]

@@ -1273,10 +1273,22 @@ int launch_wide(ispmv_plan_s *p, const FPT *x, seg::Out &o, cudaStream_t s, cons
     TRY(check_launch("x_to_f32"));
     const cudaTextureObject_t tx = TEX ? x_texture(p, p->x32, (size_t)p->n * 4, true) : 0;
     if (TEX && !tx) return launch_wide<VT, SPL, MINB, D16, false>(p, x, o, s, "stream_wide<tex: x gathered with loads>");
-    wide::stream_wide<VT, float, SPL, 0, WIDE_WARPS, MINB, D16, TEX, false, false, PFC>
-        <<<(unsigned)((p->nseg + WIDE_WARPS - 1) / WIDE_WARPS), WIDE_WARPS * 32, 0, s>>>(
-            p->slots, p->slots_pad, p->seg_slots, p->nseg, static_cast<const VT *>(p->val), p->col, p->heads, p->segh,
-            p->xw, p->x32, o, p->narrow, tx);
+    // a programmatic dependent of x_to_f32: its CTAs load their first
+    // batch while x is rounded, and wait for x_to_f32 before they gather
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)((p->nseg + WIDE_WARPS - 1) / WIDE_WARPS));
+    cfg.blockDim = dim3(WIDE_WARPS * 32);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    ISPMV_TRY(cudaLaunchKernelEx(&cfg, wide::stream_wide<VT, float, SPL, 0, WIDE_WARPS, MINB, D16, TEX, false, false, PFC>,
+                                 p->slots, p->slots_pad, p->seg_slots, p->nseg, static_cast<const VT *>(p->val),
+                                 (const UIN *)p->col, (const UIN *)p->heads, (const UIN *)p->segh, p->xw,
+                                 (const float *)p->x32, o, p->narrow, tx));
     return check_launch(name);
   } else {
     const cudaTextureObject_t tx = TEX ? x_texture(p, x, (size_t)p->n * 8, false) : 0;

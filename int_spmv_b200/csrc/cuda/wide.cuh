@@ -128,6 +128,7 @@ __device__ __forceinline__ double madd(float v, float x, double acc) { return ac
 // x32 are 16- and 8-byte aligned, two elements per thread and step.
 template <bool VEC>
 __global__ void __launch_bounds__(256) x_to_f32(size_t n, const FPT *__restrict__ x, float *__restrict__ x32) {
+  pdl_trigger();  // the product's main kernel may start loading its stream now
   const size_t stride = (size_t)gridDim.x * 256;
   size_t i = (size_t)blockIdx.x * 256 + threadIdx.x;
   if constexpr (VEC) {
@@ -371,6 +372,12 @@ __global__ void __launch_bounds__(WARPS * 32, MINB)
       for (int k = 0; k < SPL; k++) c[k] = e[k];
     }
     const unsigned bits = (__ldg(heads + (b >> 5) + ((SPL * lane) >> 5)) >> ((SPL * lane) & 31u)) & MASK;
+    if constexpr (sizeof(XT) == 4) {
+      // FP32 x is written by x_to_f32, of which this kernel is a programmatic
+      // dependent: its first batch's values and columns are loaded, now wait
+      // for that grid and its writes before the first gather
+      if (j == 0) pdl_wait();
+    }
     if constexpr (STG) {
       if (wlen) {  // first batch: the window must have landed (bounded wait)
         wlen = 0;
