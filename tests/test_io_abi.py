@@ -149,3 +149,18 @@ def test_k1_entry_points_reject_null_arrays_before_any_device_call():
     assert lib.ispmv_dev_int_k1(2, p, nul, p, p, p, p, None) == 1
     assert lib.ispmv_dev_int_k1p(0xFF, 2, nul, p, p, p, p, p, p, None) == 1
     assert lib.ispmv_dev_int_k1p(0xFF, 2, p, nul, p, p, p, p, p, None) == 1
+
+
+def test_time_main_rejects_bad_arguments_before_any_device_call():
+    """ispmv_plan_time_main checks its arguments on the host: a null plan,
+    x, y or result pointer, or fewer than one repetition, is ISPMV_ERR_ARG,
+    returned before any event is made or kernel launched (no GPU needed)."""
+    lib = load()
+    p = C.c_void_p(16)  # never dereferenced: an argument check fails first
+    nul = C.c_void_p(0)
+    ms = C.c_double()
+    assert lib.ispmv_plan_time_main(nul, p, p, 1, None, C.byref(ms)) == 1
+    assert lib.ispmv_plan_time_main(p, nul, p, 1, None, C.byref(ms)) == 1
+    assert lib.ispmv_plan_time_main(p, p, nul, 1, None, C.byref(ms)) == 1
+    assert lib.ispmv_plan_time_main(p, p, p, 0, None, C.byref(ms)) == 1
+    assert lib.ispmv_plan_time_main(p, p, p, 1, None, None) == 1
